@@ -1,0 +1,217 @@
+/* pgmg_dev.h -- C ABI of the B200 geometric multigrid library (libpgmg_b200.so).
+ *
+ * Plain pointers, sizes and status codes; no C++ or torch types.  The C++
+ * drop-in headers (include/pgmg/multigrid.hh and friends) sit on top of this
+ * ABI and keep the reference's class interface; a ctypes binding
+ * (pgmg_b200/__init__.py) calls it from Python.
+ *
+ * Scope: one process, one GPU, the whole level hierarchy resident in device
+ * memory.  Each entry point names the reference interface it replaces
+ * (file:line in chr1shr/pgmg).
+ *
+ * Conventions
+ *   - Grids are m x n x o nodes; arrays are natural order, i fastest.
+ *   - Stencils: 27 slots per point, slot (di+1)+3*(dj+1)+9*(dk+1) for the
+ *     neighbour at offset (di,dj,dk) in {-1,0,1}^3; entries outside the
+ *     point's box are zero.  Boxes ("S", region.hh:252-256) are 6 ints per
+ *     point [xd,xu,yd,yu,zd,zu] relative to the point and must lie inside
+ *     [-1,2)^3 and inside the grid on non-periodic axes.
+ *   - Host/device: every array argument may be host memory (pageable or
+ *     pinned) or device memory of the handle's GPU; the library tells them
+ *     apart through unified addressing.
+ *   - Ownership: the handle owns all device memory it allocates; caller
+ *     pointers are borrowed for the duration of the call only.  The
+ *     reference aliases external_ptr stencils for the multigrid lifetime
+ *     (region.hh:517); this library copies them at upload instead.
+ *   - Streams: all work of a handle is issued on one CUDA stream (its own,
+ *     or the one given to pgmg_dev_set_stream).  Calls returning host values
+ *     synchronise that stream.  One handle is not thread-safe; different
+ *     handles may be used from different threads.
+ *   - Errors: every call returns a pgmg_status; nothing aborts.  The C++
+ *     drop-in maps a non-zero status to p_fatal_error (common.cc:52-55)
+ *     except where the reference itself returns codes.
+ */
+#ifndef PGMG_DEV_H
+#define PGMG_DEV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..6 mirror the reference's error enum (common.hh:19-26,
+ * PGMG_FILE_ERROR..PGMG_SETUP_ERROR, shifted by one so that 0 is success). */
+typedef enum {
+    PGMG_OK = 0,
+    PGMG_ERR_FILE = 1,
+    PGMG_ERR_MEMORY = 2,
+    PGMG_ERR_INTERNAL = 3,
+    PGMG_ERR_MULTIGRID = 4,
+    PGMG_ERR_MATH = 5,
+    PGMG_ERR_SETUP = 6,
+    PGMG_ERR_ARG = 7,          /* bad argument or unsupported stencil box   */
+    PGMG_ERR_CUDA = 8,         /* a CUDA runtime call failed                */
+    PGMG_ERR_TIMEOUT = 9,      /* a bounded device wait ran out             */
+    PGMG_ERR_ADMISSION = 10,   /* request does not fit the memory cap       */
+    PGMG_ERR_UNSUPPORTED = 11, /* feature not built (e.g. periodic axes)    */
+    PGMG_ERR_NO_DEVICE = 12    /* no CUDA device visible                    */
+} pgmg_status;
+
+/* Smoother of a sweep. */
+enum {
+    PGMG_SMOOTH_MC8 = 0, /* 8-colour Gauss-Seidel, colours (i&1)|(j&1)<<1|(k&1)<<2 */
+    PGMG_SMOOTH_LEX = 1  /* lexicographic order as region.cc:367-446, by wavefronts */
+};
+
+/* Coarsest-level solver. */
+enum {
+    PGMG_COARSE_LU = 0,  /* FP64 LU with the reference's conditioning check
+                            (region_tr.cc:483-534); falls back to GS if it fails */
+    PGMG_COARSE_GS = 1   /* always pgmg_gs_exact=24 lexicographic sweeps, the
+                            reference's fallback path (region_tr.cc:557) */
+};
+
+/* Arithmetic of the V-cycle. */
+enum {
+    PGMG_FP64 = 0,       /* all-FP64, the drop-in */
+    PGMG_MIXED = 1       /* FP64 iterative refinement around an FP32 V-cycle */
+};
+
+/* Fields of a level. */
+enum {
+    PGMG_FIELD_X = 0,    /* solution x (region.hh:50-53) */
+    PGMG_FIELD_R = 1,    /* source r   (region.hh:55)    */
+    PGMG_FIELD_RES = 2   /* residual r - A x (read only) */
+};
+
+typedef struct pgmg_handle pgmg_handle;
+
+/* Grid and options.  Replaces geometry(m,n,o,x_prd,y_prd,z_prd)
+ * (geometry.cc:12-26) on one process, plus the run-time choices. */
+typedef struct {
+    int m, n, o;              /* global grid size                          */
+    int x_prd, y_prd, z_prd;  /* periodicity (non-zero: periodic)          */
+    int precision;            /* PGMG_FP64 or PGMG_MIXED                    */
+    int coarse;               /* PGMG_COARSE_LU or PGMG_COARSE_GS           */
+    int smoother;             /* default smoother of pgmg_dev_vcycle        */
+    int device;               /* CUDA device ordinal, -1 = current          */
+} pgmg_dims;
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* Plans the hierarchy (multigrid::setup_hierarchy, multigrid.cc:17-85: coarsen
+ * by (m+2)>>1 while m*n*o > 1024) and allocates every level in one device
+ * arena.  Replaces multigrid(p_class&,geometry&,comm_buffer&)
+ * (multigrid.hh:283-295) minus the problem-class callbacks. */
+pgmg_status pgmg_dev_create(const pgmg_dims *dims, pgmg_handle **out);
+/* Frees everything (multigrid::~multigrid, multigrid.cc:7-14). */
+pgmg_status pgmg_dev_destroy(pgmg_handle *h);
+/* Issue all further work of the handle on this cudaStream_t (NULL = the
+ * handle's own stream). */
+pgmg_status pgmg_dev_set_stream(pgmg_handle *h, void *cuda_stream);
+/* Waits for all work of the handle. */
+pgmg_status pgmg_dev_sync(pgmg_handle *h);
+/* Text of the last error on this handle (static storage, never NULL). */
+const char *pgmg_dev_last_error(pgmg_handle *h);
+/* Number of levels (multigrid::mlevels, multigrid.hh:135) and a level's
+ * size (region::m,n,o, region.hh:30-34). */
+pgmg_status pgmg_dev_num_levels(pgmg_handle *h, int *nlevels);
+pgmg_status pgmg_dev_level_dims(pgmg_handle *h, int level, int *mno);
+/* Device bytes held by the handle. */
+pgmg_status pgmg_dev_memory(pgmg_handle *h, size_t *bytes);
+/* Device bytes a handle with these dims would hold (admission planning). */
+pgmg_status pgmg_dev_plan_bytes(const pgmg_dims *dims, size_t *bytes);
+
+/* ---- operator set-up -------------------------------------------------- */
+
+/* Level-0 stencils, natural order, 27 slots per point; S6 (6 ints per point)
+ * may be NULL (then every box is taken as the full 27-point box, which only
+ * affects pgmg_dev_get_boxes).  Replaces region::setup_matrices
+ * (region.hh:96-101) and the top-level constructor's box pass
+ * (region.hh:492-519). */
+pgmg_status pgmg_dev_upload_level0(pgmg_handle *h, const double *coef27, const int *S6);
+/* Galerkin coarse operators A_c = (1/8) P^T A_f P on the device for every
+ * level, the coarse boxes, and the coarsest-level LU.  Replaces
+ * multigrid::compute_rats (multigrid.cc:138-152), region::fill_rat_bounds
+ * (region.cc:598-623), region::compute_rats (region.cc:629-660) and
+ * region::lu_decomposition (region_tr.cc:483-534). */
+pgmg_status pgmg_dev_build_rat(pgmg_handle *h);
+/* Whether the bottom level solves by LU (1) or by 24 sweeps (0). */
+pgmg_status pgmg_dev_lu_enabled(pgmg_handle *h, int *enabled);
+/* A level's stencils (27 slots per point) and boxes (6 ints per point). */
+pgmg_status pgmg_dev_get_coef(pgmg_handle *h, int level, double *coef27);
+pgmg_status pgmg_dev_get_boxes(pgmg_handle *h, int level, int *S6);
+
+/* ---- fields ------------------------------------------------------------ */
+
+/* Copy a field in or out, natural order, m*n*o doubles.  Replaces
+ * region::setup_x_field / setup_r_field (region.hh:110-126) and reads of
+ * reg[l]->x0 / r0.  PGMG_FIELD_RES is output only. */
+pgmg_status pgmg_dev_set_field(pgmg_handle *h, int level, int field, const double *src);
+pgmg_status pgmg_dev_get_field(pgmg_handle *h, int level, int field, double *dst);
+/* x = 0 on a level (region::clear_x_field, region.cc:1679-1682). */
+pgmg_status pgmg_dev_clear_x(pgmg_handle *h, int level);
+/* Analytic test fields (region::setup_test, region.cc:1812-1826). */
+pgmg_status pgmg_dev_setup_test(pgmg_handle *h, int level, int ca, int xfield);
+
+/* ---- hot path --------------------------------------------------------- */
+
+/* One Gauss-Seidel sweep on a level; mode != 0 adds the backward sweep
+ * (region::gauss_seidel, region.cc:355-542; multigrid::gauss_seidel,
+ * multigrid.cc:180-182). */
+pgmg_status pgmg_dev_gs(pgmg_handle *h, int level, int mode, int smoother);
+/* Residual restriction into a level from its parent, then clear that
+ * level's x (multigrid::restriction, multigrid.cc:211-224;
+ * region::restriction, region.cc:546-572). */
+pgmg_status pgmg_dev_restrict(pgmg_handle *h, int level);
+/* Trilinear interpolation of a level's x added into its parent's x
+ * (multigrid::interpolation, multigrid.cc:196-206; region.cc:576-593). */
+pgmg_status pgmg_dev_interp(pgmg_handle *h, int level);
+/* Coarsest-level solve (multigrid::solve_exact, multigrid.hh:265-267;
+ * region::solve_exact, region_tr.cc:540-558). */
+pgmg_status pgmg_dev_coarse_solve(pgmg_handle *h);
+/* One V-cycle (multigrid::v_cycle, multigrid.cc:88-106): 2+l pre- and
+ * post-sweeps on level l, coarse solve at the bottom.  smoother < 0 uses
+ * the handle's default. */
+pgmg_status pgmg_dev_vcycle(pgmg_handle *h, int mode, int smoother);
+/* Full multigrid cycle (multigrid::fmg_cycle, multigrid.cc:109-134). */
+pgmg_status pgmg_dev_fmg_cycle(pgmg_handle *h, int smoother);
+/* Sum of squared residuals and of squared sources on a level (no sqrt):
+ * region::l2_error_all (region.cc:1475-1490) and region::rhs_l2norm
+ * (region.cc:1549-1558).  Either output may be NULL. */
+pgmg_status pgmg_dev_norms(pgmg_handle *h, int level, double *res2, double *rhs2);
+
+/* ---- solves ----------------------------------------------------------- */
+
+/* multigrid::solve_v_cycles (multigrid.hh:182-219) with its mg_guide:
+ * guide.set_tol(p_scale) is applied on the first call (p_scale > 0).
+ * *result = 0 converged, 1 cycle cap, 2 NaN, as the reference returns;
+ * *res2 the final squared residual; *cycles the V-cycles run. */
+pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle *h, double p_scale, int *result,
+                                    double *res2, int *cycles);
+/* Relative-residual solve: V-cycles from the current x until
+ * sqrt(sum r^2 / sum b^2) < tol or max_cycles.  PGMG_MIXED handles run FP64
+ * iterative refinement around FP32 V-cycles.  check_every: residual check
+ * period in cycles (>= 1).  Outputs may be NULL. */
+pgmg_status pgmg_dev_solve_relres(pgmg_handle *h, double tol, int max_cycles, int check_every,
+                                  int *cycles, double *relres);
+
+/* ---- host problem generators (no GPU needed) ---------------------------- */
+
+/* Cell-centred kappa = exp(sigma*g), g a seeded Gaussian field smoothed by a
+ * Gaussian of `width` cells (0 = no smoothing) and normalised to zero mean,
+ * unit variance; (m-1)(n-1)(o-1) cells, natural order. */
+int pgmg_problem_kappa(int m, int n, int o, double sigma, uint64_t seed, double width, double *kappa);
+/* Q1 trilinear FEM stencils of -div(kappa grad u) (kappa NULL = 1) with
+ * Dirichlet fix rows on the boundary; fills coef27 and, if non-NULL, S6. */
+int pgmg_problem_q1(int m, int n, int o, const double *kappa, double *coef27, int *S6);
+/* Right-hand side: interior nodes uniform[-1,1] from the seed, boundary 0. */
+int pgmg_problem_rhs(int m, int n, int o, uint64_t seed, double *r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGMG_DEV_H */

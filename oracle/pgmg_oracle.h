@@ -1,0 +1,57 @@
+/* CPU restatement of the PGMG reference multigrid hot path (oracle).
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py as the checker.  The product never links it.
+ *
+ * Scope: one process, non-periodic axes, stencil boxes inside [-1,2)^3 (the
+ * 27-point neighbourhood), FP64.  Storage: 27 coefficient slots per point
+ * (slot (di+1)+3(dj+1)+9(dk+1), zero outside the point's box), natural order
+ * with i fastest; per-point boxes kept as 6 ints [xd,xu,yd,yu,zd,zu].
+ * Parity status: pinned against the reference compiled from its own sources
+ * (oracle/_ref/libpgmg_ref.so) by tests/test_oracle_pin.py.
+ */
+#ifndef PGMG_ORACLE_H
+#define PGMG_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc orc;
+
+/* coarse: 1 = factorise the bottom level with LU after the Galerkin build
+ * (falling back to 24 Gauss-Seidel sweeps if the conditioning check fails),
+ * 0 = always 24 Gauss-Seidel sweeps (the reference's fallback path). */
+orc* orc_create(int m,int n,int o,const int *S6,const double *c27,const double *r,
+		const double *x,int coarse);
+void orc_destroy(orc *h);
+int orc_nlevels(orc *h);
+void orc_level_dims(orc *h,int l,int *mno);
+int orc_lu_enabled(orc *h);
+void orc_get_x(orc *h,int l,double *out);
+void orc_set_x(orc *h,int l,const double *in);
+void orc_get_r(orc *h,int l,double *out);
+void orc_set_r(orc *h,int l,const double *in);
+void orc_get_S(orc *h,int l,int *out);
+void orc_get_A27(orc *h,int l,double *out);
+void orc_gauss_seidel(orc *h,int mode,int l);
+void orc_gauss_seidel_mc8(orc *h,int mode,int l);
+void orc_restriction(orc *h,int l);
+void orc_interpolation(orc *h,int l);
+void orc_solve_exact(orc *h,int l);
+void orc_v_cycle(orc *h,int mode);
+double orc_l2_error_all(orc *h,int l);
+double orc_rhs_l2norm(orc *h,int l);
+int orc_solve_v_cycles(orc *h,double p_scale,double *res,long *sweeps);
+void orc_setup_test(orc *h,int ca,int xfield,int l);
+void orc_clear_x(orc *h,int l);
+int orc_guide_pred_iters(orc *h);
+/* Plain dense LU pieces, exposed for the coarse-solver tests. */
+int orc_dgetrf(int n,double *a,int *ipiv);
+void orc_dgetrs(int n,const double *a,const int *ipiv,double *b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
