@@ -69,8 +69,11 @@ enum {
 enum {
     PGMG_COARSE_LU = 0,  /* FP64 LU with the reference's conditioning check
                             (region_tr.cc:483-534); falls back to GS if it fails */
-    PGMG_COARSE_GS = 1   /* always pgmg_gs_exact=24 lexicographic sweeps, the
+    PGMG_COARSE_GS = 1,  /* always pgmg_gs_exact=24 lexicographic sweeps, the
                             reference's fallback path (region_tr.cc:557) */
+    PGMG_COARSE_LU_EXACT = 2 /* LU solved in DGETRS order (one thread block), bit
+                            for bit the reference's solve; slower than the
+                            explicit-inverse product PGMG_COARSE_LU uses */
 };
 
 /* Arithmetic of the V-cycle. */

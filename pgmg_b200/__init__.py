@@ -1,0 +1,345 @@
+"""Python binding of libpgmg_b200.so (the C ABI in include/pgmg_dev.h).
+
+``Multigrid`` mirrors the reference's ``multigrid`` class (multigrid.hh:20-276)
+for a single process: construct with the grid size, ``setup_matrices`` with
+the level-0 stencils, ``setup_fields`` with the source, then ``v_cycle``,
+``solve_v_cycles``, per-level ``gauss_seidel`` / ``restriction`` /
+``interpolation`` / ``solve_exact`` and the norms.  All work runs in the
+CUDA library; there is no CPU fallback -- constructing a ``Multigrid`` without
+the built library or without a GPU raises ``PgmgError``.
+
+The host problem generators (``problem_kappa``, ``problem_q1``,
+``problem_rhs``) run on the CPU and need no GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpgmg_b200.so")
+
+FP64, MIXED = 0, 1
+SMOOTH_MC8, SMOOTH_LEX = 0, 1
+COARSE_LU, COARSE_GS, COARSE_LU_EXACT = 0, 1, 2
+FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
+
+_STATUS = {
+    0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
+    5: "math error", 6: "setup error", 7: "bad argument", 8: "CUDA error", 9: "timeout",
+    10: "admission rejected", 11: "unsupported", 12: "no CUDA device",
+}
+
+
+class PgmgError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        msg = f"{where}: {_STATUS.get(status, status)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+class Dims(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("o", C.c_int),
+                ("x_prd", C.c_int), ("y_prd", C.c_int), ("z_prd", C.c_int),
+                ("precision", C.c_int), ("coarse", C.c_int), ("smoother", C.c_int),
+                ("device", C.c_int)]
+
+
+_lib = None
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_VP = C.c_void_p
+
+# (name, restype, argtypes) of every exported function.
+SIGNATURES = [
+    ("pgmg_dev_create", C.c_int, [C.POINTER(Dims), C.POINTER(C.c_void_p)]),
+    ("pgmg_dev_destroy", C.c_int, [_VP]),
+    ("pgmg_dev_set_stream", C.c_int, [_VP, _VP]),
+    ("pgmg_dev_sync", C.c_int, [_VP]),
+    ("pgmg_dev_last_error", C.c_char_p, [_VP]),
+    ("pgmg_dev_num_levels", C.c_int, [_VP, C.POINTER(C.c_int)]),
+    ("pgmg_dev_level_dims", C.c_int, [_VP, C.c_int, _ip]),
+    ("pgmg_dev_memory", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
+    ("pgmg_dev_plan_bytes", C.c_int, [C.POINTER(Dims), C.POINTER(C.c_size_t)]),
+    ("pgmg_dev_upload_level0", C.c_int, [_VP, _VP, _VP]),
+    ("pgmg_dev_build_rat", C.c_int, [_VP]),
+    ("pgmg_dev_lu_enabled", C.c_int, [_VP, C.POINTER(C.c_int)]),
+    ("pgmg_dev_get_coef", C.c_int, [_VP, C.c_int, _VP]),
+    ("pgmg_dev_get_boxes", C.c_int, [_VP, C.c_int, _VP]),
+    ("pgmg_dev_set_field", C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    ("pgmg_dev_get_field", C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    ("pgmg_dev_clear_x", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_setup_test", C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
+    ("pgmg_dev_gs", C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
+    ("pgmg_dev_restrict", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_interp", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_coarse_solve", C.c_int, [_VP]),
+    ("pgmg_dev_vcycle", C.c_int, [_VP, C.c_int, C.c_int]),
+    ("pgmg_dev_fmg_cycle", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_norms", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("pgmg_dev_solve_v_cycles", C.c_int, [_VP, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("pgmg_dev_solve_relres", C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("pgmg_problem_kappa", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_double, _dp]),
+    ("pgmg_problem_q1", C.c_int, [C.c_int, C.c_int, C.c_int, _VP, _dp, _VP]),
+    ("pgmg_problem_rhs", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, _dp]),
+]
+
+
+def lib():
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PgmgError(3, "load", f"{LIB_PATH} not built; run python -m pgmg_b200.build")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------- generators
+
+def problem_kappa(m: int, n: int, o: int, sigma: float, seed: int, width: float = 8.0) -> np.ndarray:
+    """Cell-centred kappa = exp(sigma*g), (m-1)(n-1)(o-1) cells."""
+    out = np.empty((m - 1) * (n - 1) * (o - 1))
+    st = lib().pgmg_problem_kappa(m, n, o, float(sigma), int(seed), float(width), out)
+    if st:
+        raise PgmgError(st, "pgmg_problem_kappa")
+    return out
+
+
+def problem_q1(m: int, n: int, o: int, kappa: np.ndarray | None = None):
+    """Q1 FEM stencils (27 slots per point) and boxes (6 ints per point)."""
+    coef = np.empty(27 * m * n * o)
+    S = np.empty(6 * m * n * o, np.int32)
+    kp = None
+    if kappa is not None:
+        kappa = np.ascontiguousarray(kappa, np.float64)
+        kp = _ptr(kappa)
+    st = lib().pgmg_problem_q1(m, n, o, kp, coef, _ptr(S))
+    if st:
+        raise PgmgError(st, "pgmg_problem_q1")
+    return coef, S
+
+
+def problem_rhs(m: int, n: int, o: int, seed: int) -> np.ndarray:
+    out = np.empty(m * n * o)
+    st = lib().pgmg_problem_rhs(m, n, o, int(seed), out)
+    if st:
+        raise PgmgError(st, "pgmg_problem_rhs")
+    return out
+
+
+def plan_bytes(m, n, o, precision=FP64) -> int:
+    d = Dims(m, n, o, 0, 0, 0, precision, COARSE_LU, SMOOTH_MC8, -1)
+    b = C.c_size_t(0)
+    st = lib().pgmg_dev_plan_bytes(C.byref(d), C.byref(b))
+    if st:
+        raise PgmgError(st, "pgmg_dev_plan_bytes")
+    return b.value
+
+
+# ---------------------------------------------------------------- solver
+
+class Multigrid:
+    """One multigrid hierarchy on one GPU (see module docstring)."""
+
+    def __init__(self, m: int, n: int, o: int, precision: int = FP64, coarse: int = COARSE_LU,
+                 smoother: int = SMOOTH_MC8, device: int = -1, prd=(False, False, False)):
+        self.m, self.n, self.o = m, n, o
+        self.precision, self.coarse, self.smoother = precision, coarse, smoother
+        self._h = None
+        d = Dims(m, n, o, int(prd[0]), int(prd[1]), int(prd[2]), precision, coarse, smoother, device)
+        h = C.c_void_p()
+        st = lib().pgmg_dev_create(C.byref(d), C.byref(h))
+        if st:
+            raise PgmgError(st, "pgmg_dev_create")
+        self._h = h
+
+    # -- plumbing
+    def _ck(self, st, where):
+        if st:
+            detail = lib().pgmg_dev_last_error(self._h)
+            raise PgmgError(st, where, detail.decode() if detail else "")
+
+    def close(self):
+        if self._h is not None:
+            lib().pgmg_dev_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int | None):
+        self._ck(lib().pgmg_dev_set_stream(self._h, stream_ptr), "set_stream")
+
+    def sync(self):
+        self._ck(lib().pgmg_dev_sync(self._h), "sync")
+
+    @property
+    def nlevels(self) -> int:
+        v = C.c_int()
+        self._ck(lib().pgmg_dev_num_levels(self._h, C.byref(v)), "num_levels")
+        return v.value
+
+    def dims(self, level: int):
+        d = np.zeros(3, np.int32)
+        self._ck(lib().pgmg_dev_level_dims(self._h, level, d), "level_dims")
+        return tuple(int(v) for v in d)
+
+    def npts(self, level: int) -> int:
+        m, n, o = self.dims(level)
+        return m * n * o
+
+    @property
+    def memory_bytes(self) -> int:
+        b = C.c_size_t()
+        self._ck(lib().pgmg_dev_memory(self._h, C.byref(b)), "memory")
+        return b.value
+
+    # -- set-up
+    def setup_matrices(self, coef27, S6=None):
+        """Upload level-0 stencils and build every coarse operator (RAT + LU)."""
+        c = coef27 if isinstance(coef27, int) else np.ascontiguousarray(coef27, np.float64)
+        cp = c if isinstance(c, int) else _ptr(c)
+        sp = None
+        if S6 is not None:
+            S6 = np.ascontiguousarray(S6, np.int32)
+            sp = _ptr(S6)
+        self._ck(lib().pgmg_dev_upload_level0(self._h, cp, sp), "upload_level0")
+        self._ck(lib().pgmg_dev_build_rat(self._h), "build_rat")
+
+    @property
+    def lu_enabled(self) -> bool:
+        v = C.c_int()
+        self._ck(lib().pgmg_dev_lu_enabled(self._h, C.byref(v)), "lu_enabled")
+        return bool(v.value)
+
+    def get_coef(self, level: int) -> np.ndarray:
+        out = np.empty(27 * self.npts(level))
+        self._ck(lib().pgmg_dev_get_coef(self._h, level, _ptr(out)), "get_coef")
+        return out.reshape(-1, 27)
+
+    def get_boxes(self, level: int) -> np.ndarray:
+        out = np.empty(6 * self.npts(level), np.int32)
+        self._ck(lib().pgmg_dev_get_boxes(self._h, level, _ptr(out)), "get_boxes")
+        return out.reshape(-1, 6)
+
+    # -- fields
+    def set_field(self, level: int, field: int, data):
+        if isinstance(data, int):  # device pointer
+            self._ck(lib().pgmg_dev_set_field(self._h, level, field, data), "set_field")
+            return
+        a = np.ascontiguousarray(data, np.float64)
+        if a.size != self.npts(level):
+            raise ValueError("field size does not match the level")
+        self._ck(lib().pgmg_dev_set_field(self._h, level, field, _ptr(a)), "set_field")
+
+    def get_field(self, level: int, field: int, out=None) -> np.ndarray:
+        if isinstance(out, int):
+            self._ck(lib().pgmg_dev_get_field(self._h, level, field, out), "get_field")
+            return None
+        if out is None:
+            out = np.empty(self.npts(level))
+        self._ck(lib().pgmg_dev_get_field(self._h, level, field, _ptr(out)), "get_field")
+        return out
+
+    def setup_fields(self, r, x=None):
+        self.set_field(0, FIELD_R, r)
+        if x is None:
+            self.clear_x(0)
+        else:
+            self.set_field(0, FIELD_X, x)
+
+    def get_x(self, level=0):
+        return self.get_field(level, FIELD_X)
+
+    def set_x(self, level, x):
+        self.set_field(level, FIELD_X, x)
+
+    def get_r(self, level=0):
+        return self.get_field(level, FIELD_R)
+
+    def set_r(self, level, r):
+        self.set_field(level, FIELD_R, r)
+
+    def get_residual(self, level=0):
+        return self.get_field(level, FIELD_RES)
+
+    def clear_x(self, level=0):
+        self._ck(lib().pgmg_dev_clear_x(self._h, level), "clear_x")
+
+    def setup_test(self, ca: int, xfield: bool, level: int = 0):
+        self._ck(lib().pgmg_dev_setup_test(self._h, level, ca, int(xfield)), "setup_test")
+
+    # -- hot path
+    def gauss_seidel(self, mode: int = 0, level: int = 0, smoother: int | None = None):
+        s = -1 if smoother is None else smoother
+        self._ck(lib().pgmg_dev_gs(self._h, level, mode, s), "gauss_seidel")
+
+    def restriction(self, level: int):
+        self._ck(lib().pgmg_dev_restrict(self._h, level), "restriction")
+
+    def interpolation(self, level: int):
+        self._ck(lib().pgmg_dev_interp(self._h, level), "interpolation")
+
+    def solve_exact(self):
+        self._ck(lib().pgmg_dev_coarse_solve(self._h), "solve_exact")
+
+    def v_cycle(self, mode: int = 0, smoother: int | None = None):
+        s = -1 if smoother is None else smoother
+        self._ck(lib().pgmg_dev_vcycle(self._h, mode, s), "v_cycle")
+
+    def fmg_cycle(self, smoother: int | None = None):
+        s = -1 if smoother is None else smoother
+        self._ck(lib().pgmg_dev_fmg_cycle(self._h, s), "fmg_cycle")
+
+    def norms(self, level: int = 0):
+        a, b = C.c_double(), C.c_double()
+        self._ck(lib().pgmg_dev_norms(self._h, level, C.byref(a), C.byref(b)), "norms")
+        return a.value, b.value
+
+    def l2_error_all(self, level: int = 0) -> float:
+        return self.norms(level)[0]
+
+    def rhs_l2norm(self, level: int = 0) -> float:
+        return self.norms(level)[1]
+
+    def solve_v_cycles(self, p_scale: float = 0.0):
+        res = C.c_double()
+        st = C.c_int()
+        cyc = C.c_int()
+        self._ck(lib().pgmg_dev_solve_v_cycles(self._h, p_scale, C.byref(st), C.byref(res), C.byref(cyc)),
+                 "solve_v_cycles")
+        return st.value, res.value, cyc.value
+
+    def solve(self, tol: float = 1e-10, max_cycles: int = 100, check_every: int = 1):
+        cyc = C.c_int()
+        rr = C.c_double()
+        self._ck(lib().pgmg_dev_solve_relres(self._h, tol, max_cycles, check_every, C.byref(cyc), C.byref(rr)),
+                 "solve")
+        return cyc.value, rr.value

@@ -1,0 +1,794 @@
+// C ABI of the B200 multigrid library: handle and device arena, hierarchy
+// plan, operator set-up, the V-cycle engine and the solves.  See
+// include/pgmg_dev.h for the contract of every entry point.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pgmg_dev.h"
+#include "kernels_core.cuh"
+#include "kernels_setup.cuh"
+
+using namespace pgmg;
+
+namespace {
+
+constexpr int kMaxLevels = 16;      // mg_max_levels, common.hh:15
+constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
+constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
+constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
+constexpr long kMc8BlockMax = 4096;   // levels up to this size sweep 8 colours in one block
+
+struct Level {
+    LevelGeom g;
+    double *A64 = nullptr, *x64 = nullptr, *r64 = nullptr, *res64 = nullptr;
+    float *A32 = nullptr, *x32 = nullptr, *r32 = nullptr, *res32 = nullptr;
+    int8_t* S = nullptr;
+};
+
+template <class T> struct View { T *A, *x, *r, *res; };
+inline View<double> view64(Level& L) { return {L.A64, L.x64, L.r64, L.res64}; }
+inline View<float> view32(Level& L) { return {L.A32, L.x32, L.r32, L.res32}; }
+
+inline long nblk(long n, int b = kBlock) { return (n + b - 1) / b; }
+
+// Simple bump allocator over one device allocation (256-byte aligned).
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T> T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) / 256 * 256;
+        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += bytes;
+        return p;
+    }
+};
+
+}  // namespace
+
+struct pgmg_handle {
+    pgmg_dims dims{};
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    int nl = 0;
+    Level L[kMaxLevels];
+    Arena arena;
+    // coarsest level
+    long nex = 0;
+    double *M = nullptr, *Minv = nullptr, *lubuf = nullptr;
+    int *piv = nullptr, *info = nullptr;
+    int lu_ok = 0;
+    bool uploaded = false, built = false;
+    // staging and reductions
+    double* stage = nullptr;
+    size_t stage_elems = 0;
+    double* partials = nullptr;
+    double* norm_dev = nullptr;
+    double* norm_host = nullptr;  // pinned, 2 doubles
+    // mg_guide state (multigrid.hh:34-118)
+    int period = 16, iter = 16, use_avg = 0, tol_set = 0;
+    double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+pgmg_status fail(pgmg_handle* h, pgmg_status st, const char* fmt, ...) {
+    if (h) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(h->err, sizeof(h->err), fmt, ap);
+        va_end(ap);
+    }
+    return st;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(h, PGMG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define CKL() CK(cudaGetLastError())
+#define TRY(expr)                          \
+    do {                                   \
+        pgmg_status s_ = (expr);           \
+        if (s_ != PGMG_OK) return s_;      \
+    } while (0)
+
+// Hierarchy plan (multigrid::setup_hierarchy, multigrid.cc:17-85; coarse
+// sizes region.cc:14).  Periodic axes are not built yet.
+int plan_levels(const pgmg_dims& d, LevelGeom* g) {
+    int nl = 0;
+    int m = d.m, n = d.n, o = d.o;
+    g[nl++] = make_geom(m, n, o);
+    while ((long)m * n * o > 1024 && nl < kMaxLevels) {
+        m = (m + 2) >> 1; n = (n + 2) >> 1; o = (o + 2) >> 1;
+        g[nl++] = make_geom(m, n, o);
+    }
+    return nl;
+}
+
+// Lays out every buffer in the arena (or only counts bytes if base is null).
+void carve(pgmg_handle* h) {
+    Arena& a = h->arena;
+    a.used = 0;
+    bool mixed = h->dims.precision == PGMG_MIXED;
+    long maxblocks = 0;
+    for (int l = 0; l < h->nl; l++) {
+        Level& L = h->L[l];
+        const LevelGeom& g = L.g;
+        L.A64 = a.take<double>(8 * 27 * g.Nc);
+        L.x64 = a.take<double>(g.xsize);
+        L.r64 = a.take<double>(8 * g.Nc);
+        L.res64 = a.take<double>(8 * g.Nc);
+        L.S = a.take<int8_t>(6 * g.npts);
+        if (mixed) {
+            L.A32 = a.take<float>(8 * 27 * g.Nc);
+            L.x32 = a.take<float>(g.xsize);
+            L.r32 = a.take<float>(8 * g.Nc);
+            L.res32 = a.take<float>(8 * g.Nc);
+        }
+        long b = nblk((long)g.M2 * g.N2 * g.O2) * 8;
+        if (b > maxblocks) maxblocks = b;
+    }
+    long n = h->L[h->nl - 1].g.npts;
+    h->nex = n;
+    if (n < kMaxExact) {
+        h->M = a.take<double>(n * n);
+        h->Minv = a.take<double>(n * n);
+        h->lubuf = a.take<double>(n);
+        h->piv = a.take<int>(n);
+    }
+    h->info = a.take<int>(4);
+    h->partials = a.take<double>(2 * maxblocks);
+    h->norm_dev = a.take<double>(2);
+    const LevelGeom& g0 = h->L[0].g;
+    size_t coef_all = (size_t)27 * g0.npts;
+    size_t cap = (size_t)64 << 20;  // 512 MB of doubles
+    size_t st = coef_all < cap ? coef_all : cap;
+    if (st < (size_t)g0.npts) st = g0.npts;
+    if (st < (size_t)27 * g0.m * g0.n) st = (size_t)27 * g0.m * g0.n;
+    h->stage_elems = st;
+    h->stage = a.take<double>(st);
+}
+
+pgmg_status check_level(pgmg_handle* h, int level) {
+    if (!h) return PGMG_ERR_ARG;
+    if (level < 0 || level >= h->nl) return fail(h, PGMG_ERR_ARG, "level %d out of range [0,%d)", level, h->nl);
+    return PGMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle engine, templated on the storage type.
+
+template <class T> View<T> view(Level& L);
+template <> View<double> view<double>(Level& L) { return view64(L); }
+template <> View<float> view<float>(Level& L) { return view32(L); }
+
+template <class T>
+pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps = 1) {
+    Level& L = h->L[l];
+    View<T> v = view<T>(L);
+    const LevelGeom& g = L.g;
+    if (smoother == PGMG_SMOOTH_LEX) {
+        if (g.npts <= kLexBlockMax) {
+            k_gs_lex_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode);
+            CKL();
+            return PGMG_OK;
+        }
+        int np = num_planes(g);
+        for (int s = 0; s < sweeps; s++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int tt = 0; tt < np; tt++) {
+                    int t = pass ? np - 1 - tt : tt;
+                    Plane P = plane_range(g, t);
+                    long nw = (long)(P.kmax - P.kmin + 1) * P.jw;
+                    if (nw <= 0) continue;
+                    k_gs_plane<T><<<nblk(nw), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, t, P);
+                    CKL();
+                }
+        return PGMG_OK;
+    }
+    if (g.npts <= kMc8BlockMax) {
+        k_gs_mc8_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode);
+        CKL();
+        return PGMG_OK;
+    }
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    for (int s = 0; s < sweeps; s++)
+        for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+            for (int cc = 0; cc < 8; cc++) {
+                int col = pass ? 7 - cc : cc;
+                k_gs_colour<T, true><<<nblk(nc), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, col);
+                CKL();
+            }
+    return PGMG_OK;
+}
+
+template <class T>
+pgmg_status residual_level(pgmg_handle* h, int l, T* out, double* partials) {
+    Level& L = h->L[l];
+    View<T> v = view<T>(L);
+    const LevelGeom& g = L.g;
+    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    k_residual<T, T, true><<<grid, kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, out, partials);
+    CKL();
+    return PGMG_OK;
+}
+
+template <class T>
+pgmg_status restrict_level(pgmg_handle* h, int l) {
+    Level& F = h->L[l - 1];
+    Level& Cl = h->L[l];
+    View<T> vf = view<T>(F), vc = view<T>(Cl);
+    TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
+    k_restrict<T><<<nblk(Cl.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, vf.res, vc.r, vc.x);
+    CKL();
+    return PGMG_OK;
+}
+
+template <class T>
+pgmg_status interp_level(pgmg_handle* h, int l) {
+    Level& F = h->L[l - 1];
+    Level& Cl = h->L[l];
+    k_interp<T><<<nblk(F.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
+    CKL();
+    return PGMG_OK;
+}
+
+template <class T>
+pgmg_status coarse_solve_t(pgmg_handle* h) {
+    int lb = h->nl - 1;
+    Level& L = h->L[lb];
+    View<T> v = view<T>(L);
+    if (h->lu_ok) {
+        if (h->dims.coarse == PGMG_COARSE_LU_EXACT) {
+            k_lu_solve_exact<T><<<1, 1024, 0, h->stream>>>(L.g, h->M, h->piv, v.r, v.x, h->lubuf);
+        } else {
+            long thr = L.g.npts * 32;
+            k_lu_apply<T><<<nblk(thr), kBlock, 0, h->stream>>>(L.g, h->Minv, v.r, v.x);
+        }
+        CKL();
+        return PGMG_OK;
+    }
+    // region::solve_exact fallback: pgmg_gs_exact plain (mode 0) sweeps,
+    // always in the reference's lexicographic order (region_tr.cc:557).
+    return gs_level<T>(h, lb, 0, PGMG_SMOOTH_LEX, kGsExact);
+}
+
+template <class T>
+pgmg_status vcycle_t(pgmg_handle* h, int mode, int smoother) {
+    int ml = h->nl;
+    for (int i = 0; i < ml - 1; i++) {
+        TRY(gs_level<T>(h, i, mode, smoother, 2 + i));
+        TRY(restrict_level<T>(h, i + 1));
+    }
+    TRY(coarse_solve_t<T>(h));
+    for (int i = ml - 1; i > 0; i--) {
+        TRY(interp_level<T>(h, i));
+        TRY(gs_level<T>(h, i - 1, mode, smoother, 2 + i - 1));
+    }
+    return PGMG_OK;
+}
+
+// Norms of a level (FP64 data) into h->norm_host; synchronises.
+pgmg_status norms64(pgmg_handle* h, int l, double* res2, double* rhs2) {
+    Level& L = h->L[l];
+    TRY(residual_level<double>(h, l, nullptr, h->partials));
+    long nb = nblk((long)L.g.M2 * L.g.N2 * L.g.O2) * 8;
+    k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+    CKL();
+    CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (res2) *res2 = h->norm_host[0];
+    if (rhs2) *rhs2 = h->norm_host[1];
+    return PGMG_OK;
+}
+
+// One step of FP64 iterative refinement around an FP32 V-cycle:
+// r32 = b - A64 x64 (FP64 residual, stored FP32, with norms of the current
+// x), e32 = V-cycle(r32) from e32 = 0, x64 += e32.
+pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double* rhs2) {
+    Level& L0 = h->L[0];
+    const LevelGeom& g = L0.g;
+    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
+    CKL();
+    long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
+    k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+    CKL();
+    if (res2 || rhs2) {
+        CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (res2) *res2 = h->norm_host[0];
+        if (rhs2) *rhs2 = h->norm_host[1];
+    }
+    k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
+    CKL();
+    TRY(vcycle_t<float>(h, mode, smoother));
+    k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
+    CKL();
+    return PGMG_OK;
+}
+
+pgmg_status lu_setup(pgmg_handle* h) {
+    h->lu_ok = 0;
+    int lb = h->nl - 1;
+    Level& L = h->L[lb];
+    long n = L.g.npts;
+    if (n >= kMaxExact || h->dims.coarse == PGMG_COARSE_GS) return PGMG_OK;
+    CK(cudaMemsetAsync(h->M, 0, sizeof(double) * n * n, h->stream));
+    CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 4, h->stream));
+    k_lu_build<<<nblk(n * 27), kBlock, 0, h->stream>>>(L.g, L.A64, h->M);
+    CKL();
+    for (int j = 0; j < n; j++) {
+        k_lu_pivot<<<1, 1024, 0, h->stream>>>(h->M, (int)n, j, h->piv, h->info);
+        CKL();
+        long rem = n - j - 1;
+        if (rem > 0) {
+            k_lu_update<<<nblk(rem * rem), kBlock, 0, h->stream>>>(h->M, (int)n, j);
+            CKL();
+        }
+    }
+    int info = 0;
+    double u0 = 0, un = 0;
+    CK(cudaMemcpyAsync(&info, h->info, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&u0, h->M, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&un, h->M + n * n - 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // Conditioning check of region_tr.cc:524-533.
+    double hi = fabs(u0), lo = fabs(un);
+    if (info != 0 || hi == 0 || lo / hi < 2.220446049250313e-16 * 1e4) return PGMG_OK;
+    if (h->dims.coarse == PGMG_COARSE_LU) {
+        k_lu_inverse<<<nblk(n, 128), 128, 0, h->stream>>>(h->M, h->piv, (int)n, h->Minv);
+        CKL();
+    }
+    h->lu_ok = 1;
+    return PGMG_OK;
+}
+
+void guide_update(pgmg_handle* h, int extras) {
+    int diter = -1 + h->period * extras;
+    if (h->use_avg) {
+        double di = h->iter - h->iter_avg;
+        int zscore = (int)(di / sqrt(h->iter_var));
+        if (zscore > 0) diter -= zscore;
+        h->iter_avg = (1 - h->alpha) * h->iter_avg + h->alpha * h->iter;
+        h->iter_var = (1 - h->alpha) * (h->iter_var + h->alpha * di * di);
+    }
+    h->iter += diter;
+    if (h->iter < h->period) h->iter = 2 * h->period - 1;
+}
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+pgmg_status pgmg_dev_plan_bytes(const pgmg_dims* dims, size_t* bytes) {
+    if (!dims || !bytes) return PGMG_ERR_ARG;
+    if (dims->m < 2 || dims->n < 2 || dims->o < 2) return PGMG_ERR_ARG;
+    pgmg_handle tmp;
+    tmp.dims = *dims;
+    LevelGeom g[kMaxLevels];
+    tmp.nl = plan_levels(*dims, g);
+    for (int l = 0; l < tmp.nl; l++) tmp.L[l].g = g[l];
+    carve(&tmp);
+    *bytes = tmp.arena.used;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
+    if (!dims || !out) return PGMG_ERR_ARG;
+    *out = nullptr;
+    if (dims->m < 2 || dims->n < 2 || dims->o < 2) return PGMG_ERR_ARG;
+    if (dims->x_prd || dims->y_prd || dims->z_prd) return PGMG_ERR_UNSUPPORTED;
+    if (dims->precision != PGMG_FP64 && dims->precision != PGMG_MIXED) return PGMG_ERR_ARG;
+    if (dims->coarse < PGMG_COARSE_LU || dims->coarse > PGMG_COARSE_LU_EXACT) return PGMG_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PGMG_ERR_NO_DEVICE;
+    }
+    pgmg_handle* h = new pgmg_handle;
+    h->dims = *dims;
+    if (dims->device >= 0) {
+        if (dims->device >= ndev) { delete h; return PGMG_ERR_ARG; }
+        cudaSetDevice(dims->device);
+    }
+    cudaGetDevice(&h->device);
+    LevelGeom g[kMaxLevels];
+    h->nl = plan_levels(*dims, g);
+    for (int l = 0; l < h->nl; l++) h->L[l].g = g[l];
+    carve(h);  // count
+    size_t bytes = h->arena.used;
+    cudaError_t e = cudaMalloc(&h->arena.base, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return PGMG_ERR_MEMORY;
+    }
+    h->arena.size = bytes;
+    carve(h);  // assign
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&h->norm_host, 2 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        pgmg_dev_destroy(h);
+        return PGMG_ERR_CUDA;
+    }
+    h->stream = h->own;
+    if (cudaMemsetAsync(h->arena.base, 0, bytes, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        pgmg_dev_destroy(h);
+        return PGMG_ERR_CUDA;
+    }
+    *out = h;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
+    if (!h) return PGMG_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->arena.base) cudaFree(h->arena.base);
+    if (h->norm_host) cudaFreeHost(h->norm_host);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_set_stream(pgmg_handle* h, void* s) {
+    if (!h) return PGMG_ERR_ARG;
+    h->stream = s ? static_cast<cudaStream_t>(s) : h->own;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_sync(pgmg_handle* h) {
+    if (!h) return PGMG_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    return PGMG_OK;
+}
+
+const char* pgmg_dev_last_error(pgmg_handle* h) { return h ? h->err : "null handle"; }
+
+pgmg_status pgmg_dev_num_levels(pgmg_handle* h, int* nl) {
+    if (!h || !nl) return PGMG_ERR_ARG;
+    *nl = h->nl;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_level_dims(pgmg_handle* h, int level, int* mno) {
+    TRY(check_level(h, level));
+    if (!mno) return PGMG_ERR_ARG;
+    mno[0] = h->L[level].g.m; mno[1] = h->L[level].g.n; mno[2] = h->L[level].g.o;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_memory(pgmg_handle* h, size_t* bytes) {
+    if (!h || !bytes) return PGMG_ERR_ARG;
+    *bytes = h->arena.size;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const int* S6) {
+    if (!h || !coef27) return PGMG_ERR_ARG;
+    Level& L = h->L[0];
+    const LevelGeom& g = L.g;
+    // Boxes: validate on the host (region.hh:498-506 reads them per point).
+    std::vector<int8_t> s8(6 * g.npts);
+    if (S6) {
+        std::vector<int> tmp;
+        const int* sp = S6;
+        if (is_device_ptr(S6)) {
+            tmp.resize(6 * g.npts);
+            CK(cudaMemcpy(tmp.data(), S6, sizeof(int) * 6 * g.npts, cudaMemcpyDeviceToHost));
+            sp = tmp.data();
+        }
+        for (long p = 0; p < g.npts; p++) {
+            int i = (int)(p % g.m), j = (int)((p / g.m) % g.n), k = (int)(p / ((long)g.m * g.n));
+            const int* b = sp + 6 * p;
+            int c[3] = {i, j, k}, ext[3] = {g.m, g.n, g.o};
+            for (int a = 0; a < 3; a++) {
+                int lo = b[2 * a], hi = b[2 * a + 1];
+                if (lo < -1 || hi > 2 || lo >= hi || lo > 0 || hi < 1)
+                    return fail(h, PGMG_ERR_ARG, "box of point (%d,%d,%d) axis %d is [%d,%d): must contain 0 and lie in [-1,2)", i, j, k, a, lo, hi);
+                if (c[a] + lo < 0 || c[a] + hi > ext[a])
+                    return fail(h, PGMG_ERR_ARG, "box of point (%d,%d,%d) leaves the non-periodic grid on axis %d", i, j, k, a);
+                s8[6 * p + 2 * a] = (int8_t)lo;
+                s8[6 * p + 2 * a + 1] = (int8_t)hi;
+            }
+        }
+    } else {
+        for (long p = 0; p < g.npts; p++) {
+            int i = (int)(p % g.m), j = (int)((p / g.m) % g.n), k = (int)(p / ((long)g.m * g.n));
+            int c[3] = {i, j, k}, ext[3] = {g.m, g.n, g.o};
+            for (int a = 0; a < 3; a++) {
+                s8[6 * p + 2 * a] = (int8_t)(c[a] > 0 ? -1 : 0);
+                s8[6 * p + 2 * a + 1] = (int8_t)(c[a] < ext[a] - 1 ? 2 : 1);
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(L.S, s8.data(), s8.size(), cudaMemcpyHostToDevice, h->stream));
+    // Stencils, chunked by z-planes through the staging buffer.
+    long plane = 27L * g.m * g.n;
+    int kchunk = (int)(h->stage_elems / plane);
+    if (kchunk < 1) return fail(h, PGMG_ERR_INTERNAL, "staging buffer smaller than one plane");
+    for (int k0 = 0; k0 < g.o; k0 += kchunk) {
+        int k1 = k0 + kchunk < g.o ? k0 + kchunk : g.o;
+        size_t cnt = (size_t)plane * (k1 - k0);
+        CK(cudaMemcpyAsync(h->stage, coef27 + (size_t)plane * k0, cnt * sizeof(double), cudaMemcpyDefault, h->stream));
+        k_coef_to_cm<double><<<nblk((long)cnt), kBlock, 0, h->stream>>>(g, k0, k1, h->stage, L.S, L.A64);
+        CKL();
+    }
+    CK(cudaStreamSynchronize(h->stream));  // s8 and the caller's array are released on return
+    h->uploaded = true;
+    h->built = false;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->uploaded) return fail(h, PGMG_ERR_SETUP, "level-0 stencils not uploaded");
+    for (int l = 1; l < h->nl; l++) {
+        Level& F = h->L[l - 1];
+        Level& Cl = h->L[l];
+        k_rat_bounds<<<nblk(Cl.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, F.S, Cl.S);
+        CKL();
+        k_rat_fill<<<nblk(Cl.g.npts, 128), 128, 0, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+        CKL();
+    }
+    if (h->dims.precision == PGMG_MIXED)
+        for (int l = 0; l < h->nl; l++) {
+            long cnt = 8L * 27 * h->L[l].g.Nc;
+            k_cast<double, float><<<nblk(cnt), kBlock, 0, h->stream>>>(h->L[l].A64, h->L[l].A32, cnt);
+            CKL();
+        }
+    TRY(lu_setup(h));
+    CK(cudaStreamSynchronize(h->stream));
+    h->built = true;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_lu_enabled(pgmg_handle* h, int* enabled) {
+    if (!h || !enabled) return PGMG_ERR_ARG;
+    *enabled = h->lu_ok;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_get_coef(pgmg_handle* h, int level, double* coef27) {
+    TRY(check_level(h, level));
+    if (!coef27) return PGMG_ERR_ARG;
+    Level& L = h->L[level];
+    const LevelGeom& g = L.g;
+    if ((size_t)(27 * g.npts) <= h->stage_elems) {
+        k_cm_to_coef<double><<<nblk(27 * g.npts), kBlock, 0, h->stream>>>(g, L.A64, h->stage);
+        CKL();
+        CK(cudaMemcpyAsync(coef27, h->stage, sizeof(double) * 27 * g.npts, cudaMemcpyDefault, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return PGMG_OK;
+    }
+    return fail(h, PGMG_ERR_UNSUPPORTED, "level too large for read-back through the staging buffer");
+}
+
+pgmg_status pgmg_dev_get_boxes(pgmg_handle* h, int level, int* S6) {
+    TRY(check_level(h, level));
+    if (!S6) return PGMG_ERR_ARG;
+    const LevelGeom& g = h->L[level].g;
+    std::vector<int8_t> s8(6 * g.npts);
+    CK(cudaMemcpyAsync(s8.data(), h->L[level].S, s8.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> tmp(6 * g.npts);
+    for (size_t q = 0; q < s8.size(); q++) tmp[q] = s8[q];
+    CK(cudaMemcpy(S6, tmp.data(), sizeof(int) * tmp.size(), cudaMemcpyDefault));
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_set_field(pgmg_handle* h, int level, int field, const double* src) {
+    TRY(check_level(h, level));
+    if (!src || (field != PGMG_FIELD_X && field != PGMG_FIELD_R)) return PGMG_ERR_ARG;
+    Level& L = h->L[level];
+    const LevelGeom& g = L.g;
+    CK(cudaMemcpyAsync(h->stage, src, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    if (field == PGMG_FIELD_X) k_nat_to_x<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L.x64);
+    else k_nat_to_cm<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L.r64);
+    CKL();
+    CK(cudaStreamSynchronize(h->stream));
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_get_field(pgmg_handle* h, int level, int field, double* dst) {
+    TRY(check_level(h, level));
+    if (!dst) return PGMG_ERR_ARG;
+    Level& L = h->L[level];
+    const LevelGeom& g = L.g;
+    if (field == PGMG_FIELD_X) k_x_to_nat<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L.x64, h->stage);
+    else if (field == PGMG_FIELD_R) k_cm_to_nat<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L.r64, h->stage);
+    else if (field == PGMG_FIELD_RES) {
+        TRY(residual_level<double>(h, level, L.res64, nullptr));
+        k_cm_to_nat<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L.res64, h->stage);
+    } else return PGMG_ERR_ARG;
+    CKL();
+    CK(cudaMemcpyAsync(dst, h->stage, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
+    TRY(check_level(h, level));
+    k_clear_x<double><<<nblk(h->L[level].g.npts), kBlock, 0, h->stream>>>(h->L[level].g, h->L[level].x64);
+    CKL();
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_setup_test(pgmg_handle* h, int level, int ca, int xfield) {
+    TRY(check_level(h, level));
+    Level& L = h->L[level];
+    k_setup_test<double><<<nblk(L.g.npts), kBlock, 0, h->stream>>>(L.g, L.x64, L.r64, ca, xfield);
+    CKL();
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_gs(pgmg_handle* h, int level, int mode, int smoother) {
+    TRY(check_level(h, level));
+    if (smoother < 0) smoother = h->dims.smoother;
+    return gs_level<double>(h, level, mode, smoother, 1);
+}
+
+pgmg_status pgmg_dev_restrict(pgmg_handle* h, int level) {
+    TRY(check_level(h, level));
+    if (level < 1) return fail(h, PGMG_ERR_ARG, "restriction needs level >= 1");
+    return restrict_level<double>(h, level);
+}
+
+pgmg_status pgmg_dev_interp(pgmg_handle* h, int level) {
+    TRY(check_level(h, level));
+    if (level < 1) return fail(h, PGMG_ERR_ARG, "interpolation needs level >= 1");
+    return interp_level<double>(h, level);
+}
+
+pgmg_status pgmg_dev_coarse_solve(pgmg_handle* h) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    return coarse_solve_t<double>(h);
+}
+
+pgmg_status pgmg_dev_vcycle(pgmg_handle* h, int mode, int smoother) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (smoother < 0) smoother = h->dims.smoother;
+    if (h->dims.precision == PGMG_MIXED) return ir_step(h, mode, smoother, nullptr, nullptr);
+    return vcycle_t<double>(h, mode, smoother);
+}
+
+pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (smoother < 0) smoother = h->dims.smoother;
+    // multigrid::fmg_cycle (multigrid.cc:109-134), v_down = v_up = 2,
+    // v_bottom = 20 (multigrid.hh:284), mode 0.
+    int ml = h->nl;
+    for (int i = 0; i < ml - 1; i++) {
+        TRY(restrict_level<double>(h, i + 1));
+        TRY(gs_level<double>(h, i + 1, 0, smoother, 2));
+    }
+    for (int j = ml - 1; j > 0; j--) {
+        for (int i = j; i < ml - 1; i++) {
+            TRY(restrict_level<double>(h, i + 1));
+            TRY(gs_level<double>(h, i + 1, 0, smoother, 2));
+        }
+        TRY(gs_level<double>(h, ml - 1, 0, smoother, 20));
+        for (int i = ml - 1; i >= j; i--) {
+            TRY(interp_level<double>(h, i));
+            TRY(gs_level<double>(h, i - 1, 0, smoother, 2));
+        }
+    }
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_norms(pgmg_handle* h, int level, double* res2, double* rhs2) {
+    TRY(check_level(h, level));
+    return norms64(h, level, res2, rhs2);
+}
+
+pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result, double* res2, int* cycles) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (!h->tol_set) {
+        if (!(p_scale > 0)) return fail(h, PGMG_ERR_SETUP, "solve_v_cycles needs guide.set_tol (p_scale > 0)");
+        double eps = 2.220446049250313e-16;
+        h->tol = p_scale * p_scale * eps * eps * 10000;
+        h->tol_set = 1;
+    }
+    double tol = h->tol * h->dims.m;
+    tol *= h->dims.n;
+    tol *= h->dims.o;
+    int nc = 0;
+    int pred = h->iter / h->period;
+    for (int i = 0; i < pred; i++, nc++) TRY(pgmg_dev_vcycle(h, 0, -1));
+    int extra = 0, n = 0;
+    double res = 0;
+    int st = 0;
+    // The reference's loop (multigrid.hh:202-210): a NaN residual fails the
+    // "res > tol" test and leaves the loop, so its NaN branch is never taken
+    // and such a solve reports 0; this loop keeps that behaviour.
+    for (;;) {
+        TRY(norms64(h, 0, &res, nullptr));
+        if (!(res > tol && n < 100)) break;
+        if (std::isnan(res)) { st = 2; break; }
+        extra++;
+        for (int i = 0; i < extra; i++, n++, nc++) TRY(pgmg_dev_vcycle(h, 0, -1));
+    }
+    if (st == 0 && n > 100) st = 1;
+    if (st == 0) {
+        for (int i = 0; i < 2; i++, nc++) TRY(pgmg_dev_vcycle(h, 0, -1));
+        guide_update(h, extra * (extra + 1) / 2);
+    }
+    if (result) *result = st;
+    if (res2) *res2 = res;
+    if (cycles) *cycles = nc;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
+                                  double* relres) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (check_every < 1) check_every = 1;
+    int smoother = h->dims.smoother;
+    double res2 = 0, rhs2 = 0, rr = INFINITY;
+    int nc = 0;
+    if (h->dims.precision == PGMG_MIXED) {
+        Level& L0 = h->L[0];
+        const LevelGeom& g = L0.g;
+        dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+        long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
+        for (;;) {
+            // FP64 residual of the current x, stored FP32 as the correction's
+            // source, with its norms.
+            k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
+            CKL();
+            if ((nc % check_every) == 0 || nc >= max_cycles) {
+                k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+                CKL();
+                CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaStreamSynchronize(h->stream));
+                res2 = h->norm_host[0];
+                rhs2 = h->norm_host[1];
+                rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
+                if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
+            }
+            k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
+            CKL();
+            TRY(vcycle_t<float>(h, 0, smoother));
+            k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
+            CKL();
+            nc++;
+        }
+    } else {
+        for (;;) {
+            bool check = (nc % check_every) == 0 || nc >= max_cycles;
+            if (check) {
+                TRY(norms64(h, 0, &res2, &rhs2));
+                rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
+                if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
+            }
+            TRY(vcycle_t<double>(h, 0, smoother));
+            nc++;
+        }
+    }
+    if (cycles) *cycles = nc;
+    if (relres) *relres = rr;
+    return PGMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,468 @@
+// Hot-path kernels: Gauss-Seidel smoothers, residual (+norms), restriction,
+// interpolation, field movement.  All templated on the storage type T
+// (double for the FP64 V-cycle, float for the FP32 V-cycle of mixed
+// precision); EXACT selects reference-order arithmetic without fused
+// multiply-add (bitwise parity with the reference's x86-64 build).
+#pragma once
+#include "layout.cuh"
+
+namespace pgmg {
+
+constexpr int kBlock = 256;
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel point update (region.cc:367-446): terms in box order with the
+// centre skipped, x = (r - Ax) * (1/centre).  Stencil slots outside the box
+// are zero, so summing all 26 in slot order is the reference's box order.
+template <class T, bool EXACT>
+__device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ x, long xc,
+                                      const T* __restrict__ Ap, long plane, T rv) {
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        if (q == 13) continue;
+        acc = madd<EXACT, T>(acc, __ldg(Ap + q * plane), __ldg(x + xc + slot_off(g, q)));
+    }
+    T inv = T(1) / __ldg(Ap + 13 * plane);
+    if (EXACT) return mul_rn<T>(sub_rn<T>(rv, acc), inv);
+    return (rv - acc) * inv;
+}
+
+// K1: one colour of the 8-colour sweep.  Points of one colour are mutually
+// independent for a 27-point box, so the colour is one fully parallel pass;
+// the 26 neighbours read here belong to other colours and are not written
+// by this launch.  One thread per colour point; coefficient slot q of
+// consecutive threads is contiguous (structure-of-arrays per colour).
+template <class T, bool EXACT>
+__global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
+                                                      const T* __restrict__ A, int col) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (p >= nc) return;
+    int i2 = (int)(p % g.M2);
+    long t = p / g.M2;
+    int j2 = (int)(t % g.N2);
+    int k2 = (int)(t / g.N2);
+    int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+    if (i >= g.m || j >= g.n || k >= g.o) return;
+    long xc = g.xi(i, j, k);
+    const T* Ap = A + (long)col * 27 * g.Nc + p;
+    x[xc] = gs_value<T, EXACT>(g, x, xc, Ap, g.Nc, __ldg(r + (long)col * g.Nc + p));
+}
+
+// Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of
+// a 27-point box that precedes a point lexicographically lies on an earlier
+// hyperplane (offsets (-1,0,0) -> -1; (+1,-1,0) -> -1; (d,d',-1) -> <= -1)
+// and every later one on a later hyperplane, so sweeping hyperplanes in
+// order, each fully in parallel, reproduces the reference's update order.
+struct Plane {
+    int kmin, kmax, jw;
+};
+
+__host__ __device__ inline Plane plane_range(const LevelGeom& g, int t) {
+    Plane P;
+    int hi = (g.m - 1) + 2 * (g.n - 1);
+    int lo4 = t - hi;
+    P.kmin = lo4 <= 0 ? 0 : (lo4 + 3) / 4;
+    P.kmax = t / 4 < g.o - 1 ? t / 4 : g.o - 1;
+    P.jw = (g.m + 1) / 2 + 1;
+    return P;
+}
+
+__host__ __device__ inline int num_planes(const LevelGeom& g) {
+    return (g.m - 1) + 2 * (g.n - 1) + 4 * (g.o - 1) + 1;
+}
+
+// Maps work item w of hyperplane t to a grid point; false if none.
+__device__ __forceinline__ bool plane_point(const LevelGeom& g, const Plane& P, int t, int w,
+                                            int& i, int& j, int& k) {
+    k = P.kmin + w / P.jw;
+    if (k > P.kmax) return false;
+    int s = t - 4 * k;
+    int jlo4 = s - (g.m - 1);
+    int jmin = jlo4 <= 0 ? 0 : (jlo4 + 1) / 2;
+    j = jmin + w % P.jw;
+    if (j > g.n - 1 || 2 * j > s) return false;
+    i = s - 2 * j;
+    return i >= 0 && i < g.m;
+}
+
+// K2 (large levels): one hyperplane per launch.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_gs_plane(LevelGeom g, T* x, const T* __restrict__ r,
+                                                     const T* __restrict__ A, int t, Plane P) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!plane_point(g, P, t, w, i, j, k)) return;
+    long xc = g.xi(i, j, k);
+    int col = g.colour(i, j, k);
+    long c = g.cidx(i, j, k);
+    const T* Ap = A + (long)col * 27 * g.Nc + c;
+    // x is read and written in this launch, but never the same address by
+    // two threads of one hyperplane: plain loads, not the read-only path.
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        if (q == 13) continue;
+        acc = madd<true, T>(acc, Ap[q * g.Nc], x[xc + slot_off(g, q)]);
+    }
+    T inv = T(1) / Ap[13 * g.Nc];
+    x[xc] = mul_rn<T>(sub_rn<T>(r[(long)col * g.Nc + c], acc), inv);
+}
+
+// K2 (small levels): a whole level in one thread block, `sweeps` sweeps (each
+// forward, plus backward if mode), hyperplanes separated by block barriers.
+template <class T>
+__global__ void __launch_bounds__(1024) k_gs_lex_block(LevelGeom g, T* x, const T* __restrict__ r,
+                                                       const T* __restrict__ A, int sweeps, int mode) {
+    int np = num_planes(g);
+    for (int s = 0; s < sweeps; s++) {
+        for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
+            for (int tt = 0; tt < np; tt++) {
+                int t = pass ? np - 1 - tt : tt;
+                Plane P = plane_range(g, t);
+                int nw = (P.kmax - P.kmin + 1) * P.jw;
+                for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+                    int i, j, k;
+                    if (!plane_point(g, P, t, w, i, j, k)) continue;
+                    long xc = g.xi(i, j, k);
+                    int col = g.colour(i, j, k);
+                    long c = g.cidx(i, j, k);
+                    const T* Ap = A + (long)col * 27 * g.Nc + c;
+                    T acc = T(0);
+#pragma unroll
+                    for (int q = 0; q < 27; q++) {
+                        if (q == 13) continue;
+                        acc = madd<true, T>(acc, Ap[q * g.Nc], x[xc + slot_off(g, q)]);
+                    }
+                    T inv = T(1) / Ap[13 * g.Nc];
+                    x[xc] = mul_rn<T>(sub_rn<T>(r[(long)col * g.Nc + c], acc), inv);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// 8-colour sweep of a small level in one thread block.
+template <class T>
+__global__ void __launch_bounds__(1024) k_gs_mc8_block(LevelGeom g, T* x, const T* __restrict__ r,
+                                                       const T* __restrict__ A, int sweeps, int mode) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    for (int s = 0; s < sweeps; s++) {
+        for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
+            for (int cc = 0; cc < 8; cc++) {
+                int col = pass ? 7 - cc : cc;
+                for (long p = threadIdx.x; p < nc; p += blockDim.x) {
+                    int i2 = (int)(p % g.M2);
+                    long t = p / g.M2;
+                    int j2 = (int)(t % g.N2);
+                    int k2 = (int)(t / g.N2);
+                    int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+                    if (i >= g.m || j >= g.n || k >= g.o) continue;
+                    long xc = g.xi(i, j, k);
+                    const T* Ap = A + (long)col * 27 * g.Nc + p;
+                    T acc = T(0);
+#pragma unroll
+                    for (int q = 0; q < 27; q++) {
+                        if (q == 13) continue;
+                        acc = madd<true, T>(acc, Ap[q * g.Nc], x[xc + slot_off(g, q)]);
+                    }
+                    x[xc] = mul_rn<T>(sub_rn<T>(r[(long)col * g.Nc + p], acc), T(1) / Ap[13 * g.Nc]);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Block reduction of two doubles with a fixed tree (deterministic).
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) { sh[w] = a; sh[32 + w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        a = l < nw ? sh[l] : 0.0;
+        b = l < nw ? sh[32 + l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+    }
+}
+
+// K5 / residual half of K3: res = r - A x over a whole level (all 27 slots in
+// box order, region.cc:1833-1842), written colour-major to `out` (type TO),
+// with per-block partial sums of res^2 and r^2 (region.cc:1475-1490,
+// 1549-1558) when `partials` is non-null.  Grid: (blocks per colour, 8).
+template <class T, class TO, bool EXACT>
+__global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __restrict__ x,
+                                                     const T* __restrict__ r, const T* __restrict__ A,
+                                                     TO* __restrict__ out, double* __restrict__ partials) {
+    __shared__ double sh[64];
+    int col = blockIdx.y;
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    double s_res = 0, s_rhs = 0;
+    if (p < nc) {
+        int i2 = (int)(p % g.M2);
+        long t = p / g.M2;
+        int j2 = (int)(t % g.N2);
+        int k2 = (int)(t / g.N2);
+        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+        if (i < g.m && j < g.n && k < g.o) {
+            long xc = g.xi(i, j, k);
+            const T* Ap = A + (long)col * 27 * g.Nc + p;
+            T acc = T(0);
+#pragma unroll
+            for (int q = 0; q < 27; q++) acc = madd<EXACT, T>(acc, __ldg(Ap + q * g.Nc), __ldg(x + xc + slot_off(g, q)));
+            T rv = __ldg(r + (long)col * g.Nc + p);
+            T res = EXACT ? sub_rn<T>(rv, acc) : rv - acc;
+            if (out) out[(long)col * g.Nc + p] = (TO)res;
+            s_res = (double)res * (double)res;
+            s_rhs = (double)rv * (double)rv;
+        }
+    }
+    if (partials) {
+        block_sum2(s_res, s_rhs, sh);
+        if (threadIdx.x == 0) {
+            long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
+            partials[2 * b] = s_res;
+            partials[2 * b + 1] = s_rhs;
+        }
+    }
+}
+
+// Sums nb partial pairs in a fixed order into out[0], out[1].
+__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partials, long nb,
+                                                          double* __restrict__ out) {
+    __shared__ double sh[64];
+    double a = 0, b = 0;
+    for (long q = threadIdx.x; q < nb; q += blockDim.x) { a += partials[2 * q]; b += partials[2 * q + 1]; }
+    block_sum2(a, b, sh);
+    if (threadIdx.x == 0) { out[0] = a; out[1] = b; }
+}
+
+// ---------------------------------------------------------------------------
+// Restriction (region.cc:546-572, restrict_full/partial :818-912) as a gather
+// per coarse point: contributions arrive in the reference's order -- cubes in
+// scan order (z, then y, then x), fine points of a cube in x-fastest order --
+// each 0.125*w*residual with w = product of per-axis transfer weights.  The
+// reference's restrict_partial tests the x snap flag for the y axis of the
+// (ti,tj+1,tk+1) point (region.cc:888-895); that is kept, see ysnap below.
+// Also clears the coarse x (multigrid.cc:219).
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
+                                                     T* __restrict__ rc, T* __restrict__ xc) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gc.npts) return;
+    int I = (int)(q % gc.m);
+    long t = q / gc.m;
+    int J = (int)(t % gc.n);
+    int K = (int)(t / gc.n);
+    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    T acc = T(0);
+    for (int cz = K - 1; cz <= K; cz++) {
+        if (cz < 0 || cz > lz) continue;
+        bool zsn = snapped(cz, gf.o);
+        for (int cy = J - 1; cy <= J; cy++) {
+            if (cy < 0 || cy > ly) continue;
+            for (int cx = I - 1; cx <= I; cx++) {
+                if (cx < 0 || cx > lx) continue;
+                bool xsn = snapped(cx, gf.m);
+                for (int dz = 0; dz < 2; dz++) {
+                    if (dz && !has_upper(cz, gf.o)) continue;
+                    double wz = tweight(cz, dz, K, zsn);
+                    if (wz == 0.0) continue;
+                    for (int dy = 0; dy < 2; dy++) {
+                        if (dy && !has_upper(cy, gf.n)) continue;
+                        for (int dx = 0; dx < 2; dx++) {
+                            if (dx && !has_upper(cx, gf.m)) continue;
+                            bool ysn = (!dx && dy && dz) ? xsn : snapped(cy, gf.n);
+                            double w = tweight(cx, dx, I, xsn) * tweight(cy, dy, J, ysn) * wz;
+                            if (w == 0.0) continue;
+                            int fi = 2 * cx + dx, fj = 2 * cy + dy, fk = 2 * cz + dz;
+                            T rd = (T)(0.125 * w) * res[gf.ri(fi, fj, fk)];
+                            acc = add_rn<T>(acc, rd);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    rc[gc.ri(I, J, K)] = acc;
+    xc[gc.xi(I, J, K)] = T(0);
+}
+
+// Interpolation with correction add (region.cc:576-593): each fine point
+// belongs to exactly one 2x2x2 cube (C = t>>1, role t&1 per axis) and gets
+// the value interpolate_full (:752-772) or interpolate_partial (:779-810)
+// would give it -- the two differ in how some sums associate; partial is
+// used on the last cube of every row, row of every slice and slice.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
+                                                   const T* __restrict__ xcv) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gf.npts) return;
+    int i = (int)(q % gf.m);
+    long t = q / gf.m;
+    int j = (int)(t % gf.n);
+    int k = (int)(t / gf.n);
+    int Cx = i >> 1, Cy = j >> 1, Cz = k >> 1, dx = i & 1, dy = j & 1, dz = k & 1;
+    long b = gc.xi(Cx, Cy, Cz);
+    long sy = gc.mx, sz = gc.mx * gc.my;
+    // Corners outside the coarse grid read the zero halo; the formulas never
+    // use them for fine points that exist.
+    T v0 = xcv[b], v1 = xcv[b + 1], v2 = xcv[b + sy], v3 = xcv[b + sy + 1];
+    T v4 = xcv[b + sz], v5 = xcv[b + sz + 1], v6 = xcv[b + sz + sy], v7 = xcv[b + sz + sy + 1];
+    const T h = T(0.5), qq = T(0.25), e = T(0.125);
+    int role = dx | (dy << 1) | (dz << 2);
+    T val;
+    bool full = Cx < cube_last(gf.m) && Cy < cube_last(gf.n) && Cz < cube_last(gf.o);
+    if (full) {
+        switch (role) {
+            case 0: val = v0; break;
+            case 1: val = h * (v0 + v1); break;
+            case 2: val = h * (v0 + v2); break;
+            case 3: val = qq * (((v0 + v1) + v2) + v3); break;
+            case 4: val = h * (v0 + v4); break;
+            case 5: val = qq * ((v0 + v1) + (v4 + v5)); break;
+            case 6: val = qq * (((v0 + v2) + v4) + v6); break;
+            default: val = e * (((((((v0 + v1) + v2) + v3) + (v4 + v5)) + v6) + v7)); break;
+        }
+    } else {
+        bool xs = snapped(Cx, gf.m), ys = snapped(Cy, gf.n), zs = snapped(Cz, gf.o);
+        switch (role) {
+            case 0: val = v0; break;
+            case 1: val = xs ? v1 : h * (v0 + v1); break;
+            case 2: val = ys ? v2 : h * (v0 + v2); break;
+            case 4: val = zs ? v4 : h * (v0 + v4); break;
+            case 5: val = zs ? (xs ? v5 : h * (v4 + v5)) : (xs ? h * (v1 + v5) : qq * (((v0 + v1) + v4) + v5)); break;
+            case 6: val = zs ? (ys ? v6 : h * (v4 + v6)) : (ys ? h * (v2 + v6) : qq * (((v0 + v2) + v4) + v6)); break;
+            default: {
+                T t2 = ys ? (xs ? v3 : h * (v2 + v3)) : (xs ? h * (v1 + v3) : qq * (((v0 + v1) + v2) + v3));
+                if (role == 3) { val = t2; break; }
+                T t3 = ys ? (xs ? v7 : h * (v6 + v7)) : (xs ? h * (v5 + v7) : qq * (((v4 + v5) + v6) + v7));
+                val = zs ? t3 : h * (t3 + t2);
+            }
+        }
+    }
+    long xf_i = gf.xi(i, j, k);
+    xf[xf_i] = xf[xf_i] + val;
+}
+
+// ---------------------------------------------------------------------------
+// Field movement between natural order (double, caller side) and the level
+// layout.  Grid over natural points.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_nat_to_x(LevelGeom g, const double* __restrict__ src, T* __restrict__ x) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    x[g.xi(i, j, k)] = (T)src[q];
+}
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_x_to_nat(LevelGeom g, const T* __restrict__ x, double* __restrict__ dst) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    dst[q] = (double)x[g.xi(i, j, k)];
+}
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_nat_to_cm(LevelGeom g, const double* __restrict__ src, T* __restrict__ r) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    r[g.ri(i, j, k)] = (T)src[q];
+}
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_cm_to_nat(LevelGeom g, const T* __restrict__ r, double* __restrict__ dst) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    dst[q] = (double)r[g.ri(i, j, k)];
+}
+
+// Stencils of planes [k0,k1) from natural 27-slot doubles (src holds exactly
+// those planes) into the colour-major layout; slots outside the point's box
+// (if boxes are given) are stored as zero, since the reference never reads them.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_coef_to_cm(LevelGeom g, int k0, int k1, const double* __restrict__ src,
+                                                       const int8_t* __restrict__ S, T* __restrict__ A) {
+    long npl = (long)g.m * g.n * (k1 - k0);
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= npl * 27) return;
+    long pt = q / 27;
+    int s = (int)(q % 27);
+    int i = (int)(pt % g.m); long t = pt / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n) + k0;
+    double v = src[q];
+    if (S) {
+        const int8_t* b = S + 6 * g.pi(i, j, k);
+        int di = s % 3 - 1, dj = (s / 3) % 3 - 1, dk = s / 9 - 1;
+        if (di < b[0] || di >= b[1] || dj < b[2] || dj >= b[3] || dk < b[4] || dk >= b[5]) v = 0.0;
+    }
+    A[g.ai(i, j, k, s)] = (T)v;
+}
+
+// Colour-major stencils back to natural 27-slot doubles.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_cm_to_coef(LevelGeom g, const T* __restrict__ A, double* __restrict__ dst) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts * 27) return;
+    long pt = q / 27;
+    int s = (int)(q % 27);
+    int i = (int)(pt % g.m); long t = pt / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    dst[q] = (double)A[g.ai(i, j, k, s)];
+}
+
+// Interior of x set to zero (region::clear_x_field, region.cc:1679-1682).
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_clear_x(LevelGeom g, T* __restrict__ x) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    x[g.xi(i, j, k)] = T(0);
+}
+
+// region::setup_test (region.cc:1812-1826), one process.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_setup_test(LevelGeom g, T* x, T* r, int ca, int xfield) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    T v;
+    switch (ca) {
+        case 0: v = i; break;
+        case 1: v = j; break;
+        case 2: v = k; break;
+        case 3: v = k + j + i; break;
+        case 4: v = 0; break;
+        case 5: v = (i == 7 && j == 7 && k == 7) ? 1 : 0; break;
+        default: v = 1;
+    }
+    if (xfield) x[g.xi(i, j, k)] = v; else r[g.ri(i, j, k)] = v;
+}
+
+// Elementwise casts used by mixed precision.
+template <class TI, class TO>
+__global__ void __launch_bounds__(kBlock) k_cast(const TI* __restrict__ in, TO* __restrict__ out, long n) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q < n) out[q] = (TO)in[q];
+}
+
+// x64 += x32 over the interior (FP64 update of iterative refinement).
+__global__ void __launch_bounds__(kBlock) k_add_correction(LevelGeom g, double* __restrict__ x64,
+                                                           const float* __restrict__ e32) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    long c = g.xi(i, j, k);
+    x64[c] = x64[c] + (double)e32[c];
+}
+
+}  // namespace pgmg

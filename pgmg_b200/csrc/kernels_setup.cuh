@@ -1,0 +1,323 @@
+// Set-up kernels: Galerkin coarse operators (RAT) and their boxes, and the
+// coarsest-level dense LU.  FP64 throughout.
+#pragma once
+#include "layout.cuh"
+
+namespace pgmg {
+
+// Per-axis list of the fine points (cube C, role d, weight w, A_mul factor f)
+// that transfer to coarse index I, in scan order (cube I-1 first, lower role
+// first).  At most 3 entries.
+struct AxisList {
+    int n;
+    int C[3], d[3];
+    double w[3], f[3];
+};
+
+__device__ inline AxisList axis_list(int I, int ma) {
+    AxisList L;
+    L.n = 0;
+    int last = cube_last(ma);
+    for (int C = I - 1; C <= I; C++) {
+        if (C < 0 || C > last) continue;
+        bool sn = snapped(C, ma);
+        for (int d = 0; d < 2; d++) {
+            if (d && !has_upper(C, ma)) continue;
+            double w = tweight(C, d, I, sn);
+            if (w == 0.0) continue;
+            L.C[L.n] = C; L.d[L.n] = d; L.w[L.n] = w;
+            L.f[L.n] = (d && !sn) ? 0.5 : 1.0;
+            L.n++;
+        }
+    }
+    return L;
+}
+
+// fill_rat_bounds (region.cc:598-623; rat_bound_full/partial :916-1003;
+// b_red :1105-1110; b_ex :1276-1283): coarse box = [0,1)^3 extended by the
+// grid_map'ed global box of every fine point that transfers to the coarse
+// point.  One thread per coarse point; boxes as int8[6] natural order.
+__global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGeom gc, const int8_t* __restrict__ Sf,
+                                                    int8_t* __restrict__ Sc) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gc.npts) return;
+    int I = (int)(q % gc.m); long t = q / gc.m; int J = (int)(t % gc.n); int K = (int)(t / gc.n);
+    int s[6] = {0, 1, 0, 1, 0, 1};
+    AxisList X = axis_list(I, gf.m), Y = axis_list(J, gf.n), Z = axis_list(K, gf.o);
+    for (int c = 0; c < Z.n; c++)
+        for (int b = 0; b < Y.n; b++)
+            for (int a = 0; a < X.n; a++) {
+                int ti = 2 * X.C[a] + X.d[a], tj = 2 * Y.C[b] + Y.d[b], tk = 2 * Z.C[c] + Z.d[c];
+                const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                int lo, hi;
+                lo = fs[0] + ti; hi = fs[1] + ti; grid_map(lo, hi, gf.m);
+                s[0] = min(s[0], lo - I); s[1] = max(s[1], hi - I);
+                lo = fs[2] + tj; hi = fs[3] + tj; grid_map(lo, hi, gf.n);
+                s[2] = min(s[2], lo - J); s[3] = max(s[3], hi - J);
+                lo = fs[4] + tk; hi = fs[5] + tk; grid_map(lo, hi, gf.o);
+                s[4] = min(s[4], lo - K); s[5] = max(s[5], hi - K);
+            }
+    for (int u = 0; u < 6; u++) Sc[6 * q + u] = (int8_t)s[u];
+}
+
+// compute_rats (region.cc:629-660) as a gather per coarse point, in the
+// reference's accumulation order: fine points in cube scan order (z, y, x
+// cubes; x-fastest roles); for each, A_red (:1117-1166) forms
+// At(J) = sum_u 0.125*A_f(t,u)*w(u->J) over u in igrid_map's range cropped to
+// t's box (kk, jj, ii order), A_mul scales it by 1/2 per non-snapped upper
+// axis, and A_add (:1173-1180) adds it to this coarse point's row.  Products
+// by powers of two are exact, sums are rounded one by one (no fused
+// multiply-add), so the result matches the reference bit for bit.
+// Grid: one thread per coarse point.  Output: colour-major coarse stencils.
+__global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
+                                                  const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gc.npts) return;
+    int I = (int)(q % gc.m); long t = q / gc.m; int J = (int)(t % gc.n); int K = (int)(t / gc.n);
+    double acc[27];
+#pragma unroll
+    for (int s = 0; s < 27; s++) acc[s] = 0.0;
+    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    for (int cz = K - 1; cz <= K; cz++) {
+        if (cz < 0 || cz > lz) continue;
+        for (int cy = J - 1; cy <= J; cy++) {
+            if (cy < 0 || cy > ly) continue;
+            for (int cx = I - 1; cx <= I; cx++) {
+                if (cx < 0 || cx > lx) continue;
+                for (int dz = 0; dz < 2; dz++) {
+                    if (dz && !has_upper(cz, gf.o)) continue;
+                    bool zsn = snapped(cz, gf.o);
+                    if (tweight(cz, dz, K, zsn) == 0.0) continue;
+                    for (int dy = 0; dy < 2; dy++) {
+                        if (dy && !has_upper(cy, gf.n)) continue;
+                        bool ysn = snapped(cy, gf.n);
+                        if (tweight(cy, dy, J, ysn) == 0.0) continue;
+                        for (int dx = 0; dx < 2; dx++) {
+                            if (dx && !has_upper(cx, gf.m)) continue;
+                            bool xsn = snapped(cx, gf.m);
+                            if (tweight(cx, dx, I, xsn) == 0.0) continue;
+                            double fac = ((dx && !xsn) ? 0.5 : 1.0) * ((dy && !ysn) ? 0.5 : 1.0) *
+                                         ((dz && !zsn) ? 0.5 : 1.0);
+                            int ti = 2 * cx + dx, tj = 2 * cy + dy, tk = 2 * cz + dz;
+                            const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                            int B[6] = {fs[0] + ti, fs[1] + ti, fs[2] + tj, fs[3] + tj, fs[4] + tk, fs[5] + tk};
+                            int St[6] = {B[0], B[1], B[2], B[3], B[4], B[5]};
+                            grid_map(St[0], St[1], gf.m);
+                            grid_map(St[2], St[3], gf.n);
+                            grid_map(St[4], St[5], gf.o);
+                            int fcol = gf.colour(ti, tj, tk);
+                            const double* fa = Af + (long)fcol * 27 * gf.Nc + gf.cidx(ti, tj, tk);
+                            for (int vk = St[4]; vk < St[5]; vk++) {
+                                int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
+                                for (int vj = St[2]; vj < St[3]; vj++) {
+                                    int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n);
+                                    for (int vi = St[0]; vi < St[1]; vi++) {
+                                        int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m);
+                                        double At = 0.0;
+                                        for (int kk = lk; kk < uk; kk++) {
+                                            double kfac = kk == ck ? 1.0 : 0.5;
+                                            for (int jj = lj; jj < uj; jj++) {
+                                                double jkfac = jj == cj ? kfac : 0.5 * kfac;
+                                                for (int ii = li; ii < ui; ii++) {
+                                                    int slot = (ii - ti + 1) + 3 * (jj - tj + 1) + 9 * (kk - tk + 1);
+                                                    double term = __dmul_rn(__dmul_rn(0.125, fa[slot * gf.Nc]),
+                                                                            ii == ci ? jkfac : 0.5 * jkfac);
+                                                    At = __dadd_rn(At, term);
+                                                }
+                                            }
+                                        }
+                                        int s = (vi - I + 1) + 3 * (vj - J + 1) + 9 * (vk - K + 1);
+                                        acc[s] = __dadd_rn(acc[s], __dmul_rn(At, fac));
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    int col = gc.colour(I, J, K);
+    long c = gc.cidx(I, J, K);
+#pragma unroll
+    for (int s = 0; s < 27; s++) Ac[((long)col * 27 + s) * gc.Nc + c] = acc[s];
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level: dense column-major matrix Aexact[row + col*n] from the
+// level's stencils (region_tr.cc:489-508, non-periodic: no wrap needed).
+__global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, double* __restrict__ M) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long n = g.npts;
+    if (q >= n * 27) return;
+    long row = q / 27;
+    int s = (int)(q % 27);
+    int i = (int)(row % g.m); long t = row / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int ii = i + s % 3 - 1, jj = j + (s / 3) % 3 - 1, kk = k + s / 9 - 1;
+    if (ii < 0 || jj < 0 || kk < 0 || ii >= g.m || jj >= g.n || kk >= g.o) return;
+    M[row + g.pi(ii, jj, kk) * n] = A[g.ai(i, j, k, s)];
+}
+
+// Column j of the LU factorisation with partial pivoting, the same
+// operations as DGETF2 (and the oracle's restatement): pivot = first row of
+// largest |a_ij|, i >= j; swap rows across the whole matrix; scale the
+// sub-column by 1/a_jj.  info[0] = first zero pivot (1-based).  One block.
+__global__ void __launch_bounds__(1024) k_lu_pivot(double* __restrict__ M, int n, int j, int* __restrict__ piv,
+                                                   int* __restrict__ info) {
+    __shared__ double sv[32];
+    __shared__ int si[32];
+    __shared__ int sp;
+    double best = -1.0;
+    int bi = n;
+    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+        double v = fabs(M[i + (long)j * n]);
+        if (v > best) { best = v; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_down_sync(0xffffffffu, best, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sv[w] = best; si[w] = bi; }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        best = l < nw ? sv[l] : -1.0;
+        bi = l < nw ? si[l] : n;
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, best, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (l == 0) sp = bi;
+    }
+    __syncthreads();
+    int p = sp < n ? sp : j;  // all-NaN column: keep the diagonal
+    if (threadIdx.x == 0) piv[j] = p + 1;
+    double apj = M[p + (long)j * n];
+    if (apj != 0.0) {
+        if (p != j)
+            for (int c = threadIdx.x; c < n; c += blockDim.x) {
+                double tmp = M[j + (long)c * n];
+                M[j + (long)c * n] = M[p + (long)c * n];
+                M[p + (long)c * n] = tmp;
+            }
+        __syncthreads();
+        double r = 1.0 / M[j + (long)j * n];
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i + (long)j * n] = __dmul_rn(M[i + (long)j * n], r);
+    } else if (threadIdx.x == 0 && info[0] == 0) {
+        info[0] = j + 1;
+    }
+}
+
+// Rank-1 update of the trailing block after column j.  Thread per element.
+__global__ void __launch_bounds__(256) k_lu_update(double* __restrict__ M, int n, int j) {
+    long rem = n - j - 1;
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= rem * rem) return;
+    int i = j + 1 + (int)(q % rem);
+    int k = j + 1 + (int)(q / rem);
+    double u = M[j + (long)k * n];
+    if (u != 0.0) M[i + (long)k * n] = __dsub_rn(M[i + (long)k * n], __dmul_rn(M[i + (long)j * n], u));
+}
+
+// Inverse from the factors, row-major Minv[i*n + c]: thread c solves
+// A x = e_c with the recorded interchanges, unit-lower forward and upper
+// backward substitution (column-oriented, as DGETRS), working in column c
+// of the output so that a warp's accesses are contiguous.
+__global__ void __launch_bounds__(128) k_lu_inverse(const double* __restrict__ M, const int* __restrict__ piv,
+                                                    int n, double* __restrict__ Minv) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    for (int i = 0; i < n; i++) Minv[(long)i * n + c] = (i == c) ? 1.0 : 0.0;
+    for (int i = 0; i < n; i++) {
+        int p = piv[i] - 1;
+        if (p != i) {
+            double t = Minv[(long)i * n + c];
+            Minv[(long)i * n + c] = Minv[(long)p * n + c];
+            Minv[(long)p * n + c] = t;
+        }
+    }
+    for (int j = 0; j < n; j++) {
+        double xj = Minv[(long)j * n + c];
+        if (xj != 0.0)
+            for (int i = j + 1; i < n; i++)
+                Minv[(long)i * n + c] = __dsub_rn(Minv[(long)i * n + c], __dmul_rn(xj, M[i + (long)j * n]));
+    }
+    for (int j = n - 1; j >= 0; j--) {
+        double xj = Minv[(long)j * n + c];
+        if (xj != 0.0) {
+            xj = xj / M[j + (long)j * n];
+            Minv[(long)j * n + c] = xj;
+            for (int i = 0; i < j; i++)
+                Minv[(long)i * n + c] = __dsub_rn(Minv[(long)i * n + c], __dmul_rn(xj, M[i + (long)j * n]));
+        }
+    }
+}
+
+// Coarse solve by the explicit inverse: x(i) = sum_c Minv[i][c] * r(c), one
+// warp per row, FP64 accumulation, fixed reduction tree.  r is the level's
+// colour-major source (type T), x its halo'd solution.
+template <class T>
+__global__ void __launch_bounds__(256) k_lu_apply(LevelGeom g, const double* __restrict__ Minv,
+                                                  const T* __restrict__ r, T* __restrict__ x) {
+    int n = (int)g.npts;
+    int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int l = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0.0;
+    for (int c = l; c < n; c += 32) {
+        int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+        s = fma(Minv[(long)row * n + c], (double)r[g.ri(i, j, k)], s);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (l == 0) {
+        int i = row % g.m, t = row / g.m, j = t % g.n, k = t / g.n;
+        x[g.xi(i, j, k)] = (T)s;
+    }
+}
+
+// Coarse solve in DGETRS order (one block): the interchanges, then
+// column-oriented forward and backward substitution, each column's updates
+// in parallel -- the same operations as the oracle's restatement, so the
+// result matches it bit for bit.  buf: n doubles of scratch.
+template <class T>
+__global__ void __launch_bounds__(1024) k_lu_solve_exact(LevelGeom g, const double* __restrict__ M,
+                                                         const int* __restrict__ piv, const T* __restrict__ r,
+                                                         T* __restrict__ x, double* __restrict__ b) {
+    int n = (int)g.npts;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+        b[c] = (double)r[g.ri(i, j, k)];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < n; i++) {
+            int p = piv[i] - 1;
+            if (p != i) { double t = b[i]; b[i] = b[p]; b[p] = t; }
+        }
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+        double xj = b[j];
+        if (xj != 0.0)
+            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) b[i] = __dsub_rn(b[i], __dmul_rn(xj, M[i + (long)j * n]));
+        __syncthreads();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+        double xj = b[j];
+        if (xj != 0.0) {
+            xj = xj / M[j + (long)j * n];
+            for (int i = threadIdx.x; i < j; i += blockDim.x) b[i] = __dsub_rn(b[i], __dmul_rn(xj, M[i + (long)j * n]));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && xj != 0.0) b[j] = xj;
+        __syncthreads();
+    }
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+        x[g.xi(i, j, k)] = (T)b[c];
+    }
+}
+
+}  // namespace pgmg

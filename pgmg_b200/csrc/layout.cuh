@@ -1,0 +1,127 @@
+// Device layout of one multigrid level and the index arithmetic shared by
+// every kernel.
+//
+//  * x   (solution, region.hh:50-53): natural order with a one-point zero halo
+//        on every side, (m+2)(n+2)(o+2) values; x(i,j,k) at
+//        (i+1) + mx*((j+1) + my*(k+1)), mx = m+2, my = n+2.  The halo is never
+//        written, so every stencil slot can be read without bounds checks.
+//  * r   (source, region.hh:55) and the residual scratch: colour-major,
+//        [8][Nc]; colour c = (i&1) | (j&1)<<1 | (k&1)<<2, in-colour index
+//        p = ((k>>1)*N2 + (j>>1))*M2 + (i>>1) with M2 = (m+1)/2 etc.
+//  * A   (stencils, region.hh:57-59): colour-major structure-of-arrays,
+//        [8][27][Nc]: slot q of every point of colour c is contiguous, so a
+//        colour sweep streams 27 dense planes.  Slot q = (di+1)+3(dj+1)+9(dk+1);
+//        zero outside the point's box (region.hh:252-256).
+//  * S   (boxes): natural order, 6 int8 per point, relative [xd,xu,yd,yu,zd,zu];
+//        used only during set-up (coarse boxes, parity read-back).
+// Nc is M2*N2*O2 rounded up to a multiple of 64, so every plane starts on a
+// 256-byte boundary in FP32 and FP64.  Colour sub-grid entries that fall
+// outside the grid (odd sizes) hold zero stencils and are never updated.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pgmg {
+
+struct LevelGeom {
+    int m, n, o;     // grid size
+    int M2, N2, O2;  // colour sub-grid size, (m+1)/2 ...
+    long Nc;         // padded points per colour
+    long mx, my;     // halo'd x strides: m+2, n+2
+    long xsize;      // (m+2)(n+2)(o+2)
+    long npts;       // m*n*o
+
+    __host__ __device__ inline long xi(int i, int j, int k) const {
+        return (i + 1) + mx * ((j + 1) + my * (long)(k + 1));
+    }
+    __host__ __device__ inline int colour(int i, int j, int k) const {
+        return (i & 1) | ((j & 1) << 1) | ((k & 1) << 2);
+    }
+    __host__ __device__ inline long cidx(int i, int j, int k) const {
+        return ((long)(k >> 1) * N2 + (j >> 1)) * M2 + (i >> 1);
+    }
+    // Index of (i,j,k) in an [8][Nc] array.
+    __host__ __device__ inline long ri(int i, int j, int k) const {
+        return (long)colour(i, j, k) * Nc + cidx(i, j, k);
+    }
+    // Index of slot q of (i,j,k) in an [8][27][Nc] array.
+    __host__ __device__ inline long ai(int i, int j, int k, int q) const {
+        return ((long)colour(i, j, k) * 27 + q) * Nc + cidx(i, j, k);
+    }
+    __host__ __device__ inline long pi(int i, int j, int k) const {
+        return i + (long)m * (j + (long)n * k);
+    }
+};
+
+inline LevelGeom make_geom(int m, int n, int o) {
+    LevelGeom g;
+    g.m = m; g.n = n; g.o = o;
+    g.M2 = (m + 1) / 2; g.N2 = (n + 1) / 2; g.O2 = (o + 1) / 2;
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    g.Nc = (nc + 63) / 64 * 64;
+    g.mx = m + 2; g.my = n + 2;
+    g.xsize = (long)(m + 2) * (n + 2) * (o + 2);
+    g.npts = (long)m * n * o;
+    return g;
+}
+
+// Per-axis transfer geometry between a fine axis of size ma and its coarse
+// axis (ma+2)>>1 (region.cc:14), as rt_scan_grid/slice/row walk it on one
+// process (region.cc:665-746): cubes C = 0..last; the lower point 2C always
+// exists; the upper point 2C+1 exists unless C is the last cube of an odd
+// axis; on an even axis the last cube's upper point (ma-1) "snaps" onto
+// coarse C+1 with weight 1 (mask bits 4/32/256).
+__host__ __device__ inline int cube_last(int ma) { int sm = (ma + 2) >> 1; return (ma & 1) ? sm - 1 : sm - 2; }
+__host__ __device__ inline bool has_upper(int C, int ma) { return 2 * C + 1 < ma; }
+__host__ __device__ inline bool snapped(int C, int ma) { return !(ma & 1) && C == cube_last(ma); }
+
+// Weight of fine role d (0 lower, 1 upper) of cube C onto coarse index I,
+// 0 if the fine point does not transfer to I.
+__host__ __device__ inline double tweight(int C, int d, int I, bool snap) {
+    if (!d) return C == I ? 1.0 : 0.0;
+    if (snap) return C + 1 == I ? 1.0 : 0.0;
+    return (C == I || C + 1 == I) ? 0.5 : 0.0;
+}
+
+// grid_map, non-periodic (region.cc:1209-1216).
+__host__ __device__ inline void grid_map(int& lo, int& hi, int ma) {
+    lo = (!(ma & 1) && lo == ma - 1 ? lo + 1 : lo) >> 1;
+    hi = (hi + 2) >> 1;
+}
+
+// igrid_map, non-periodic, with the crop to the stencil box (region.cc:1243-1258).
+__host__ __device__ inline int igrid_map(int& lo, int& hi, int blo, int bhi, int i, int ma) {
+    int j = i << 1;
+    if (ma & 1) { lo = j == 0 ? 0 : j - 1; hi = j == ma - 1 ? ma : j + 2; }
+    else if (j == ma) { lo = ma - 1; hi = ma; j = ma - 1; }
+    else { lo = j == 0 ? 0 : j - 1; hi = j == ma - 2 ? ma - 1 : j + 2; }
+    if (lo < blo) lo = blo;
+    if (hi > bhi) hi = bhi;
+    return j;
+}
+
+// Arithmetic helpers: EXACT = round every product and sum separately, as the
+// reference's x86-64 build does (no fused multiply-add), so results match it
+// bit for bit; otherwise fused multiply-add.
+template <class T> __device__ inline T mul_rn(T a, T b);
+template <> __device__ inline double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
+template <> __device__ inline float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
+template <class T> __device__ inline T add_rn(T a, T b);
+template <> __device__ inline double add_rn<double>(double a, double b) { return __dadd_rn(a, b); }
+template <> __device__ inline float add_rn<float>(float a, float b) { return __fadd_rn(a, b); }
+template <class T> __device__ inline T sub_rn(T a, T b);
+template <> __device__ inline double sub_rn<double>(double a, double b) { return __dsub_rn(a, b); }
+template <> __device__ inline float sub_rn<float>(float a, float b) { return __fsub_rn(a, b); }
+
+template <bool EXACT, class T> __device__ inline T madd(T acc, T a, T b) {
+    if (EXACT) return add_rn<T>(acc, mul_rn<T>(a, b));
+    return fma(a, b, acc);
+}
+
+// Offset of slot q in the halo'd x array.
+__host__ __device__ inline long slot_off(const LevelGeom& g, int q) {
+    int di = q % 3 - 1, dj = (q / 3) % 3 - 1, dk = q / 9 - 1;
+    return di + g.mx * (dj + g.my * dk);
+}
+
+}  // namespace pgmg

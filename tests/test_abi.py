@@ -1,0 +1,82 @@
+"""C-ABI library: loads on a machine without a GPU, exports every symbol
+include/pgmg_dev.h declares, host generators are deterministic, and the
+device entry points fail with a status (not a crash) without a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pgmg_b200 as P
+from tests.conftest import ROOT, gpu_available
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "pgmg_dev.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pgmg_(?:dev|problem)_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(P.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    bound = {name for name, _, _ in P.SIGNATURES}
+    assert set(syms) <= bound, set(syms) - bound
+
+
+def test_generators_deterministic():
+    a = P.problem_kappa(9, 10, 11, 1.0, 3)
+    b = P.problem_kappa(9, 10, 11, 1.0, 3)
+    c = P.problem_kappa(9, 10, 11, 1.0, 4)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    g = np.log(a)
+    assert abs(g.mean()) < 1e-12 and abs(g.std() - 1.0) < 1e-12
+    r1 = P.problem_rhs(9, 10, 11, 3)
+    assert np.array_equal(r1, P.problem_rhs(9, 10, 11, 3))
+    r3 = r1.reshape(11, 10, 9)
+    assert np.all(r3[0] == 0) and np.all(r3[:, 0] == 0) and np.all(r3[:, :, -1] == 0)
+    inner = r3[1:-1, 1:-1, 1:-1]
+    assert inner.min() >= -1 and inner.max() <= 1 and inner.std() > 0.4
+
+
+def test_q1_constant_stencil():
+    m = 9
+    coef, S = P.problem_q1(m, m, m)
+    h = 1.0 / (m - 1)
+    c = coef.reshape(-1, 27)
+    st = c[4 + 9 * (4 + 9 * 4)].reshape(3, 3, 3)
+    ndiff = np.add.outer(np.add.outer([1, 0, 1], [1, 0, 1]), [1, 0, 1])  # differing coordinates
+    expect = np.choose(ndiff, [8 / 3, 0.0, -1 / 6, -1 / 12]) * h
+    np.testing.assert_allclose(st, expect, rtol=1e-15, atol=1e-17)
+    assert abs(st.sum()) < 1e-15
+    # Boundary rows: one positive fix entry, box [0,1)^3.
+    assert np.count_nonzero(c[0]) == 1 and c[0, 13] == pytest.approx(8 / 3 * h)
+    assert list(S.reshape(-1, 6)[0]) == [0, 1, 0, 1, 0, 1]
+
+
+def test_plan_bytes_and_levels():
+    b65 = P.plan_bytes(65, 65, 65)
+    b257 = P.plan_bytes(257, 257, 257)
+    bm = P.plan_bytes(257, 257, 257, P.MIXED)
+    assert 0 < b65 < b257 < bm
+    # 27 FP64 stencils per point dominate.
+    assert b257 > 27 * 8 * 257 ** 3
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU path")
+def test_create_without_gpu_raises():
+    with pytest.raises(P.PgmgError) as e:
+        P.Multigrid(9, 9, 9)
+    assert e.value.status == 12
+
+
+def test_create_rejects_bad_args():
+    d = P.Dims(1, 9, 9, 0, 0, 0, 0, 0, 0, -1)
+    h = C.c_void_p()
+    assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 7
+    d = P.Dims(9, 9, 9, 1, 0, 0, 0, 0, 0, -1)
+    assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 11

@@ -1,0 +1,150 @@
+"""Pins the CPU oracle (oracle/pgmg_oracle.c) to the reference.
+
+* Known-answer tests from the reference's own test programs:
+  lapack_test.cc:36-49 (2x2 LU solve), mg_test.cc:32-33 with
+  region.cc:1819 (trilinear interpolation of x=j is exact).
+* The restatement against the reference compiled from its own sources
+  (oracle/_ref/libpgmg_ref.so): every level's boxes and Galerkin stencils,
+  restriction, interpolation, lexicographic Gauss-Seidel (forward and
+  symmetric), the coarse solve, V-cycles and solve_v_cycles, compared bit
+  for bit, on odd, even and anisotropic grids.
+* The LU restatement against LAPACK (scipy's dgetrf/dgetrs).
+No GPU needed.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from oracle.pyoracle import Oracle, Reference, oracle_lib, ref_available
+from tests.helpers import q1_problem, simple_problem
+
+needs_ref = pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+
+SIZES = [(17, 17, 17), (16, 17, 18), (20, 33, 9), (12, 12, 12), (33, 33, 33), (34, 18, 10)]
+
+
+def test_lapack_kat():
+    # lapack_test.cc:36-49: A = {1,1,2,1} column-major, b = {3,7}.
+    A = np.array([1.0, 1.0, 2.0, 1.0])
+    b = np.array([3.0, 7.0])
+    piv = np.zeros(2, np.int32)
+    assert oracle_lib().orc_dgetrf(2, A, piv) == 0
+    oracle_lib().orc_dgetrs(2, A, piv, b)
+    np.testing.assert_allclose(b, [11.0, -4.0], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("n", [2, 37, 200])
+def test_lu_restatement_vs_lapack(n):
+    rng = np.random.default_rng(n)
+    M = rng.standard_normal((n, n)) + n * 0.1 * np.eye(n)
+    b = rng.standard_normal(n)
+    a = np.asfortranarray(M).ravel(order="F").copy()
+    piv = np.zeros(n, np.int32)
+    assert oracle_lib().orc_dgetrf(n, a, piv) == 0
+    x = b.copy()
+    oracle_lib().orc_dgetrs(n, a, piv, x)
+    lu, p = sla.lu_factor(M)
+    xr = sla.lu_solve((lu, p), b)
+    assert np.abs(x - xr).max() <= 1e-13 * np.abs(xr).max()
+    # Pivot sequences agree (LAPACK's are 0-based in scipy).
+    assert np.array_equal(piv - 1, p)
+
+
+def test_lu_zero_matrix_reports_info():
+    a = np.zeros(9)
+    piv = np.zeros(3, np.int32)
+    assert oracle_lib().orc_dgetrf(3, a, piv) == 1
+
+
+def test_interpolation_of_linear_field_is_exact():
+    # mg_test.cc:32-33: x=j on level 3 of a 65^3 hierarchy, interpolated to level 2.
+    coef, S, r = simple_problem(65, 65, 65)
+    O = Oracle(65, 65, 65, S, coef, r, coarse=False)
+    assert O.nlevels == 4
+    O.clear_x(2)
+    O.setup_test(1, True, 3)
+    O.interpolation(3)
+    m, n, o = O.dims(2)
+    j = np.broadcast_to(np.arange(n)[None, :, None], (o, n, m)).ravel()
+    np.testing.assert_array_equal(O.get_x(2), j / 2.0)
+
+
+@needs_ref
+@pytest.mark.parametrize("mno", SIZES)
+def test_oracle_matches_reference_bitwise(mno):
+    m, n, o = mno
+    coef, S, r = q1_problem(m, n, o, sigma=1.0, seed=sum(mno))
+    R = Reference(m, n, o, S, coef, r)
+    O = Oracle(m, n, o, S, coef, r, coarse=R.lu_enabled)
+    assert O.nlevels == R.nlevels
+    assert O.lu_enabled == R.lu_enabled
+    for l in range(R.nlevels):
+        assert O.dims(l) == R.dims(l)
+        assert np.array_equal(O.get_S(l), R.get_S(l))
+        assert np.array_equal(O.get_A27(l), R.get_A27(l))
+    rng = np.random.default_rng(7)
+    for l in range(1, R.nlevels):
+        xf = rng.standard_normal(R.npts(l - 1))
+        for h in (R, O):
+            h.set_x(l - 1, xf)
+            h.restriction(l)
+        assert np.array_equal(O.get_r(l), R.get_r(l))
+        assert np.array_equal(O.get_x(l), R.get_x(l))  # cleared by restriction
+        xc = rng.standard_normal(R.npts(l))
+        for h in (R, O):
+            h.set_x(l, xc)
+            h.set_x(l - 1, xf)
+            h.interpolation(l)
+        assert np.array_equal(O.get_x(l - 1), R.get_x(l - 1))
+    for l in range(R.nlevels):
+        for mode in (0, 1):
+            x0 = rng.standard_normal(R.npts(l))
+            for h in (R, O):
+                h.set_x(l, x0)
+                h.gauss_seidel(mode, l)
+            assert np.array_equal(O.get_x(l), R.get_x(l))
+    for h in (R, O):
+        h.set_x(0, np.zeros(R.npts(0)))
+    for it in range(3):
+        R.v_cycle(0)
+        O.v_cycle(0)
+        assert np.array_equal(O.get_x(0), R.get_x(0))
+        assert O.l2_error_all() == R.l2_error_all()
+    R.v_cycle(1)
+    O.v_cycle(1)
+    assert np.array_equal(O.get_x(0), R.get_x(0))
+    assert O.rhs_l2norm() == R.rhs_l2norm()
+
+
+@needs_ref
+def test_solve_v_cycles_matches_reference():
+    m = n = o = 33
+    coef, S, r = q1_problem(m, n, o, sigma=1.0, seed=5)
+    R = Reference(m, n, o, S, coef, r)
+    O = Oracle(m, n, o, S, coef, r, coarse=R.lu_enabled)
+    for rep in range(2):
+        for h in (R, O):
+            h.set_x(0, np.zeros(m * n * o))
+        sr = R.solve_v_cycles(8.0 / 3 / 32)
+        so = O.solve_v_cycles(8.0 / 3 / 32)
+        assert sr == so
+        assert R.guide_pred_iters() == O.guide_pred_iters()
+        assert np.array_equal(O.get_x(0), R.get_x(0))
+
+
+@needs_ref
+def test_reference_problem_simple_bitwise():
+    # The reference's own problem class and driver sizes (gs_parallel-like
+    # standalone sweeps on level 0, then V-cycles).
+    m = n = o = 25
+    coef, S, r = simple_problem(m, n, o)
+    R = Reference(m, n, o, S, coef, r)
+    O = Oracle(m, n, o, S, coef, r, coarse=R.lu_enabled)
+    for s in range(3):
+        R.gauss_seidel(0, 0)
+        O.gauss_seidel(0, 0)
+        assert R.l2_error_all() == O.l2_error_all()
+    for it in range(2):
+        R.v_cycle(0)
+        O.v_cycle(0)
+    assert np.array_equal(O.get_x(0), R.get_x(0))
