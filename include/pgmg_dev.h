@@ -118,6 +118,10 @@ pgmg_status pgmg_dev_set_stream(pgmg_handle *h, void *cuda_stream);
 pgmg_status pgmg_dev_sync(pgmg_handle *h);
 /* Text of the last error on this handle (static storage, never NULL). */
 const char *pgmg_dev_last_error(pgmg_handle *h);
+/* Kernels the handle has launched so far (all of them this library's own). */
+pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
+/* Default smoother of pgmg_dev_vcycle and the solves. */
+pgmg_status pgmg_dev_set_smoother(pgmg_handle *h, int smoother);
 /* Number of levels (multigrid::mlevels, multigrid.hh:135) and a level's
  * size (region::m,n,o, region.hh:30-34). */
 pgmg_status pgmg_dev_num_levels(pgmg_handle *h, int *nlevels);

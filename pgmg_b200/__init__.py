@@ -61,6 +61,8 @@ SIGNATURES = [
     ("pgmg_dev_set_stream", C.c_int, [_VP, _VP]),
     ("pgmg_dev_sync", C.c_int, [_VP]),
     ("pgmg_dev_last_error", C.c_char_p, [_VP]),
+    ("pgmg_dev_launch_count", C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    ("pgmg_dev_set_smoother", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_num_levels", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("pgmg_dev_level_dims", C.c_int, [_VP, C.c_int, _ip]),
     ("pgmg_dev_memory", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
@@ -199,6 +201,16 @@ class Multigrid:
 
     def sync(self):
         self._ck(lib().pgmg_dev_sync(self._h), "sync")
+
+    @property
+    def launches(self) -> int:
+        v = C.c_longlong()
+        self._ck(lib().pgmg_dev_launch_count(self._h, C.byref(v)), "launch_count")
+        return v.value
+
+    def set_smoother(self, smoother: int):
+        self._ck(lib().pgmg_dev_set_smoother(self._h, smoother), "set_smoother")
+        self.smoother = smoother
 
     @property
     def nlevels(self) -> int:

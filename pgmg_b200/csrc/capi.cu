@@ -70,6 +70,7 @@ struct pgmg_handle {
     // mg_guide state (multigrid.hh:34-118)
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;
     double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;
+    long long launches = 0;  // kernels this handle has launched
     char err[512] = {0};
 };
 
@@ -90,7 +91,11 @@ pgmg_status fail(pgmg_handle* h, pgmg_status st, const char* fmt, ...) {
         cudaError_t e_ = (call);                                                              \
         if (e_ != cudaSuccess) return fail(h, PGMG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
-#define CKL() CK(cudaGetLastError())
+#define CKL()             \
+    do {                  \
+        h->launches++;    \
+        CK(cudaGetLastError()); \
+    } while (0)
 #define TRY(expr)                          \
     do {                                   \
         pgmg_status s_ = (expr);           \
@@ -460,6 +465,18 @@ pgmg_status pgmg_dev_sync(pgmg_handle* h) {
 }
 
 const char* pgmg_dev_last_error(pgmg_handle* h) { return h ? h->err : "null handle"; }
+
+pgmg_status pgmg_dev_launch_count(pgmg_handle* h, long long* n) {
+    if (!h || !n) return PGMG_ERR_ARG;
+    *n = h->launches;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_set_smoother(pgmg_handle* h, int smoother) {
+    if (!h || (smoother != PGMG_SMOOTH_MC8 && smoother != PGMG_SMOOTH_LEX)) return PGMG_ERR_ARG;
+    h->dims.smoother = smoother;
+    return PGMG_OK;
+}
 
 pgmg_status pgmg_dev_num_levels(pgmg_handle* h, int* nl) {
     if (!h || !nl) return PGMG_ERR_ARG;

@@ -139,16 +139,19 @@ int pgmg_problem_q1(int m, int n, int o, const double* kappa, double* coef27, in
                 for (int q = 0; q < 27; q++) c[q] = 0;
                 bool interior = i > 0 && i < m - 1 && j > 0 && j < n - 1 && k > 0 && k < o - 1;
                 if (interior) {
-                    // The 8 cells around the node; (a,b,e) is the node's corner in the cell.
-                    for (int e = 0; e < 2; e++)
-                        for (int b = 0; b < 2; b++)
-                            for (int a = 0; a < 2; a++) {
-                                double ke = h * kap(i - 1 + a, j - 1 + b, k - 1 + e);
+                    // The 8 cells around the node: cell (i+ca, j+cb, k+ce) with
+                    // ca,cb,ce in {-1,0}; the node is that cell's local corner
+                    // (-ca,-cb,-ce), the cell's other corner (aa,bb,ee) is the
+                    // node at offset (aa+ca, bb+cb, ee+ce).
+                    for (int ce = -1; ce <= 0; ce++)
+                        for (int cb = -1; cb <= 0; cb++)
+                            for (int ca = -1; ca <= 0; ca++) {
+                                double ke = h * kap(i + ca, j + cb, k + ce);
                                 for (int ee = 0; ee < 2; ee++)
                                     for (int bb = 0; bb < 2; bb++)
                                         for (int aa = 0; aa < 2; aa++) {
-                                            int diff = (aa != a) + (bb != b) + (ee != e);
-                                            int q = (aa - a + 1) + 3 * (bb - b + 1) + 9 * (ee - e + 1);
+                                            int diff = (aa != -ca) + (bb != -cb) + (ee != -ce);
+                                            int q = (aa + ca + 1) + 3 * (bb + cb + 1) + 9 * (ee + ce + 1);
                                             c[q] += ke * khat[diff];
                                         }
                             }

