@@ -237,7 +237,7 @@ def run_ours(a):
 
     def solve_once(H):
         H.clear_x(0)
-        return H.solve(a.tol, 100, 1)
+        return H.solve(a.tol, 100, 0)
 
     # --- device-resident solves -------------------------------------------
     for _ in range(a.warmup):
@@ -275,7 +275,7 @@ def run_ours(a):
     for _ in range(a.steps):
         G.set_field(0, P.FIELD_R, hr.data_ptr())
         G.clear_x(0)
-        G.solve(a.tol, 100, 1)
+        G.solve(a.tol, 100, 0)
         G.get_field(0, P.FIELD_X, hx.data_ptr())
     e1.record(stream)
     torch.cuda.synchronize()
@@ -316,7 +316,7 @@ def run_ours(a):
         torch.cuda.synchronize()
         mms = max_over_ranks(m0.elapsed_time(m1) / a.steps)
         xm = Gm.get_x(0)
-        xd = G.get_x(0)
+        xd = hx.numpy()  # FP64 solution of the last end-to-end step
         mixed = {"value": mms / 1e3, "unit": UNIT, "cycles": mc, "relres": mr,
                  "speedup_vs_fp64": ms / mms,
                  "max_rel_diff_vs_fp64_solution": float(np.abs(xm - xd).max() / np.abs(xd).max())}

@@ -201,7 +201,8 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle *h, double p_scale, int *result,
 /* Relative-residual solve: V-cycles from the current x until
  * sqrt(sum r^2 / sum b^2) < tol or max_cycles.  PGMG_MIXED handles run FP64
  * iterative refinement around FP32 V-cycles.  check_every: residual check
- * period in cycles (>= 1).  Outputs may be NULL. */
+ * period in cycles (>= 1), or 0 for an adaptive schedule that predicts the
+ * remaining cycles from the observed reduction factor.  Outputs may be NULL. */
 pgmg_status pgmg_dev_solve_relres(pgmg_handle *h, double tol, int max_cycles, int check_every,
                                   int *cycles, double *relres);
 

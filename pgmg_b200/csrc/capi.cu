@@ -756,52 +756,77 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result,
     return PGMG_OK;
 }
 
+// Residual-check schedule of the relative-residual solve.  check_every >= 1:
+// every that many cycles.  check_every == 0: adaptive -- after two checks the
+// per-cycle reduction factor is estimated from the last two residuals and
+// the solve runs one cycle fewer than predicted before checking again, so a
+// converged solve rarely pays for more than one check past the prediction.
+struct CheckPlan {
+    int every;
+    int last_n = -1, prev_n = -1;
+    double last_r = 0, prev_r = 0;
+    int next(int nc, double tol) const {
+        if (every >= 1) return nc + every;
+        if (prev_n < 0 || last_r <= 0 || prev_r <= 0) return nc + 1;
+        double rho = pow(last_r / prev_r, 1.0 / (last_n - prev_n));
+        if (!(rho > 0) || rho >= 0.9) return nc + 1;
+        int need = (int)ceil(log(tol / last_r) / log(rho));
+        return nc + (need > 2 ? need - 1 : 1);
+    }
+    void record(int nc, double r) { prev_n = last_n; prev_r = last_r; last_n = nc; last_r = r; }
+};
+
 pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
                                   double* relres) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
-    if (check_every < 1) check_every = 1;
+    if (check_every < 0) check_every = 1;
     int smoother = h->dims.smoother;
     double res2 = 0, rhs2 = 0, rr = INFINITY;
-    int nc = 0;
-    if (h->dims.precision == PGMG_MIXED) {
-        Level& L0 = h->L[0];
-        const LevelGeom& g = L0.g;
-        dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
-        long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
-        for (;;) {
+    int nc = 0, next_check = 0;
+    CheckPlan plan;
+    plan.every = check_every;
+    Level& L0 = h->L[0];
+    const LevelGeom& g = L0.g;
+    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
+    bool mixed = h->dims.precision == PGMG_MIXED;
+    for (;;) {
+        bool check = nc >= next_check || nc >= max_cycles;
+        if (mixed) {
             // FP64 residual of the current x, stored FP32 as the correction's
-            // source, with its norms.
-            k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
+            // source (and reduced to the norms when checking).
+            k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32,
+                                                                              check ? h->partials : nullptr);
             CKL();
-            if ((nc % check_every) == 0 || nc >= max_cycles) {
-                k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
-                CKL();
-                CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-                CK(cudaStreamSynchronize(h->stream));
-                res2 = h->norm_host[0];
-                rhs2 = h->norm_host[1];
-                rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
-                if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
-            }
+        } else if (check) {
+            k_residual<double, double, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, nullptr,
+                                                                               h->partials);
+            CKL();
+        }
+        if (check) {
+            k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+            CKL();
+            CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            res2 = h->norm_host[0];
+            rhs2 = h->norm_host[1];
+            rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
+            if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
+            plan.record(nc, rr);
+            next_check = plan.next(nc, tol);
+            if (next_check > max_cycles) next_check = max_cycles;
+        }
+        if (mixed) {
             k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
             CKL();
             TRY(vcycle_t<float>(h, 0, smoother));
             k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
             CKL();
-            nc++;
-        }
-    } else {
-        for (;;) {
-            bool check = (nc % check_every) == 0 || nc >= max_cycles;
-            if (check) {
-                TRY(norms64(h, 0, &res2, &rhs2));
-                rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
-                if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
-            }
+        } else {
             TRY(vcycle_t<double>(h, 0, smoother));
-            nc++;
         }
+        nc++;
     }
     if (cycles) *cycles = nc;
     if (relres) *relres = rr;
