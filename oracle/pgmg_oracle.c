@@ -47,6 +47,7 @@ struct orc {
 	int period,iter,use_avg,tol_set;
 	double iter_avg,iter_var,alpha,tol;
 	int v_down,v_up,v_bottom;
+	int smoother;  /* 0 = lexicographic (reference), 1 = 8-colour */
 };
 
 static inline long xi(const olev *L,int i,int j,int k) {
@@ -437,8 +438,14 @@ void orc_interpolation(orc *h,int l) {
 	}
 }
 
+static void gs_any(orc *h,int mode,int l) {
+	if(h->smoother) orc_gauss_seidel_mc8(h,mode,l); else orc_gauss_seidel(h,mode,l);
+}
+
+void orc_set_smoother(orc *h,int mc8) {h->smoother=mc8?1:0;}
+
 /* region::solve_exact (region_tr.cc:540-558): LU solve if enabled, else
- * pgmg_gs_exact plain sweeps. */
+ * pgmg_gs_exact plain sweeps (of the selected smoother). */
 void orc_solve_exact(orc *h,int l) {
 	olev *L=&h->L[l];
 	if(l==h->nl-1&&h->lu_ok) {
@@ -446,20 +453,20 @@ void orc_solve_exact(orc *h,int l) {
 		orc_dgetrs((int)L->N,h->LU,h->piv,h->buf);
 		const double *p=h->buf;
 		for(int k=0;k<L->o;k++) for(int j=0;j<L->n;j++) for(int i=0;i<L->m;i++) L->x[xi(L,i,j,k)]=*(p++);
-	} else for(int q=0;q<ORC_GS_EXACT;q++) orc_gauss_seidel(h,0,l);
+	} else for(int q=0;q<ORC_GS_EXACT;q++) gs_any(h,0,l);
 }
 
 /* multigrid::v_cycle (multigrid.cc:88-106). */
 void orc_v_cycle(orc *h,int mode) {
 	int i,q,ml=h->nl;
 	for(i=0;i<ml-1;i++) {
-		for(q=0;q<h->v_down+i;q++) orc_gauss_seidel(h,mode,i);
+		for(q=0;q<h->v_down+i;q++) gs_any(h,mode,i);
 		orc_restriction(h,i+1);
 	}
 	orc_solve_exact(h,ml-1);
 	for(i=ml-1;i>0;i--) {
 		orc_interpolation(h,i);
-		for(q=0;q<h->v_up+i-1;q++) orc_gauss_seidel(h,mode,i-1);
+		for(q=0;q<h->v_up+i-1;q++) gs_any(h,mode,i-1);
 	}
 }
 

@@ -36,6 +36,9 @@ void orc_get_S(orc *h,int l,int *out);
 void orc_get_A27(orc *h,int l,double *out);
 void orc_gauss_seidel(orc *h,int mode,int l);
 void orc_gauss_seidel_mc8(orc *h,int mode,int l);
+/* Smoother of orc_v_cycle and of the coarse fallback sweeps: 0 = the
+ * reference's lexicographic Gauss-Seidel (default), 1 = 8-colour. */
+void orc_set_smoother(orc *h,int mc8);
 void orc_restriction(orc *h,int l);
 void orc_interpolation(orc *h,int l);
 void orc_solve_exact(orc *h,int l);

@@ -176,6 +176,8 @@ def oracle_lib():
         lib.orc_get_A27.argtypes = [C.c_void_p, C.c_int, _dp]
         lib.orc_gauss_seidel_mc8.restype = None
         lib.orc_gauss_seidel_mc8.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        lib.orc_set_smoother.restype = None
+        lib.orc_set_smoother.argtypes = [C.c_void_p, C.c_int]
         lib.orc_dgetrf.restype = C.c_int
         lib.orc_dgetrf.argtypes = [C.c_int, _dp, _ip]
         lib.orc_dgetrs.restype = None
@@ -229,6 +231,9 @@ class Oracle(_Base):
 
     def gauss_seidel_mc8(self, mode=0, level=0):
         self.lib.orc_gauss_seidel_mc8(self.h, mode, level)
+
+    def set_smoother(self, mc8: bool):
+        self.lib.orc_set_smoother(self.h, int(mc8))
 
 
 class Reference(_Base):

@@ -25,6 +25,7 @@ FP64, MIXED = 0, 1
 SMOOTH_MC8, SMOOTH_LEX = 0, 1
 COARSE_LU, COARSE_GS, COARSE_LU_EXACT = 0, 1, 2
 FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
+OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE = 1, 2, 3
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -63,6 +64,8 @@ SIGNATURES = [
     ("pgmg_dev_last_error", C.c_char_p, [_VP]),
     ("pgmg_dev_launch_count", C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     ("pgmg_dev_set_smoother", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_set_option", C.c_int, [_VP, C.c_int, C.c_longlong]),
+    ("pgmg_dev_get_option", C.c_int, [_VP, C.c_int, C.POINTER(C.c_longlong)]),
     ("pgmg_dev_num_levels", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("pgmg_dev_level_dims", C.c_int, [_VP, C.c_int, _ip]),
     ("pgmg_dev_memory", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
@@ -206,6 +209,14 @@ class Multigrid:
     def launches(self) -> int:
         v = C.c_longlong()
         self._ck(lib().pgmg_dev_launch_count(self._h, C.byref(v)), "launch_count")
+        return v.value
+
+    def set_option(self, key: int, value: int):
+        self._ck(lib().pgmg_dev_set_option(self._h, key, int(value)), "set_option")
+
+    def get_option(self, key: int) -> int:
+        v = C.c_longlong()
+        self._ck(lib().pgmg_dev_get_option(self._h, key, C.byref(v)), "get_option")
         return v.value
 
     def set_smoother(self, smoother: int):

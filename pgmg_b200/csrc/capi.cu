@@ -5,9 +5,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/pgmg_dev.h"
+#include "kernels_coarse.cuh"
 #include "kernels_core.cuh"
 #include "kernels_setup.cuh"
 
@@ -19,7 +21,9 @@ constexpr int kMaxLevels = 16;      // mg_max_levels, common.hh:15
 constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
 constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
 constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
-constexpr long kMc8BlockMax = 4096;   // levels up to this size sweep 8 colours in one block
+constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
+constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
+constexpr int kClusterThreads = 512;
 
 struct Level {
     LevelGeom g;
@@ -71,6 +75,16 @@ struct pgmg_handle {
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;
     double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;
     long long launches = 0;  // kernels this handle has launched
+    bool x0_zero = true;     // level-0 x known to be zero (cleared, not written since)
+    double last_rho = 0;     // per-cycle residual reduction seen by the last solve
+    // Captured V-cycles, by [float][mode][smoother].
+    cudaGraphExec_t vgraph[2][2][2] = {};
+    long long vgraph_nodes[2][2][2] = {};
+    bool use_graphs = true;
+    // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
+    // first level it handles.
+    int cluster_size = 0;
+    int coarse_first = 0;
     char err[512] = {0};
 };
 
@@ -244,7 +258,7 @@ pgmg_status interp_level(pgmg_handle* h, int l) {
 }
 
 template <class T>
-pgmg_status coarse_solve_t(pgmg_handle* h) {
+pgmg_status coarse_solve_t(pgmg_handle* h, int smoother) {
     int lb = h->nl - 1;
     Level& L = h->L[lb];
     View<T> v = view<T>(L);
@@ -258,23 +272,128 @@ pgmg_status coarse_solve_t(pgmg_handle* h) {
         CKL();
         return PGMG_OK;
     }
-    // region::solve_exact fallback: pgmg_gs_exact plain (mode 0) sweeps,
-    // always in the reference's lexicographic order (region_tr.cc:557).
-    return gs_level<T>(h, lb, 0, PGMG_SMOOTH_LEX, kGsExact);
+    // region::solve_exact fallback: pgmg_gs_exact plain (mode 0) sweeps of
+    // the cycle's smoother (region_tr.cc:557; the reference's own smoother is
+    // the lexicographic one).
+    return gs_level<T>(h, lb, 0, smoother, kGsExact);
 }
 
 template <class T>
+pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
+    CoarsePlan<T> P;
+    P.first = first;
+    P.nl = h->nl;
+    P.lu_ok = h->lu_ok;
+    P.Minv = h->Minv;
+    for (int l = 0; l < h->nl; l++) {
+        View<T> v = view<T>(h->L[l]);
+        P.g[l] = h->L[l].g;
+        P.A[l] = v.A; P.x[l] = v.x; P.r[l] = v.r; P.res[l] = v.res;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->cluster_size, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = h->cluster_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, P, mode));
+    h->launches++;
+    return PGMG_OK;
+}
+
+// Largest usable cluster (16, non-portable, else 8) for the coarse cycle.
+template <class T>
+int probe_cluster(int size) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(size, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (size > 8 && cudaFuncSetAttribute(k_coarse_cycle<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_coarse_cycle<T>, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// One V-cycle (multigrid::v_cycle, multigrid.cc:88-106).  With the 8-colour
+// smoother the levels from h->coarse_first down run as one cluster kernel;
+// the LU-exact coarse solve and the lexicographic smoother use the grid
+// kernels on every level.
+template <class T>
 pgmg_status vcycle_t(pgmg_handle* h, int mode, int smoother) {
     int ml = h->nl;
-    for (int i = 0; i < ml - 1; i++) {
+    bool cl = smoother == PGMG_SMOOTH_MC8 && h->cluster_size > 0 && h->dims.coarse != PGMG_COARSE_LU_EXACT;
+    int lc = cl ? h->coarse_first : ml;
+    int top = lc < ml ? lc : ml - 1;
+    for (int i = 0; i < top; i++) {
         TRY(gs_level<T>(h, i, mode, smoother, 2 + i));
         TRY(restrict_level<T>(h, i + 1));
     }
-    TRY(coarse_solve_t<T>(h));
-    for (int i = ml - 1; i > 0; i--) {
+    if (lc < ml) TRY(launch_coarse<T>(h, lc, mode));
+    else TRY(coarse_solve_t<T>(h, smoother));
+    for (int i = top; i > 0; i--) {
         TRY(interp_level<T>(h, i));
         TRY(gs_level<T>(h, i - 1, mode, smoother, 2 + i - 1));
     }
+    return PGMG_OK;
+}
+
+void drop_graphs(pgmg_handle* h) {
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int c = 0; c < 2; c++)
+                if (h->vgraph[a][b][c]) {
+                    cudaGraphExecDestroy(h->vgraph[a][b][c]);
+                    h->vgraph[a][b][c] = nullptr;
+                }
+}
+
+// One V-cycle as a CUDA graph: the launch sequence of vcycle_t is captured
+// once per (precision, mode, smoother) and replayed, so the several hundred
+// small launches of the coarse levels cost no host launch overhead.
+template <class T>
+pgmg_status run_vcycle(pgmg_handle* h, int mode, int smoother) {
+    if (!h->use_graphs) return vcycle_t<T>(h, mode, smoother);
+    int a = std::is_same<T, float>::value ? 1 : 0, b = mode ? 1 : 0, c = smoother == PGMG_SMOOTH_LEX ? 1 : 0;
+    cudaGraphExec_t& ex = h->vgraph[a][b][c];
+    if (!ex) {
+        long long before = h->launches;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        pgmg_status st = vcycle_t<T>(h, mode, smoother);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+        if (st != PGMG_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        CK(e);
+        e = cudaGraphInstantiate(&ex, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ex = nullptr;
+            return fail(h, PGMG_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        }
+        h->vgraph_nodes[a][b][c] = h->launches - before;
+        h->launches = before;
+    }
+    CK(cudaGraphLaunch(ex, h->stream));
+    h->launches += h->vgraph_nodes[a][b][c];
     return PGMG_OK;
 }
 
@@ -312,7 +431,7 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
     }
     k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
     CKL();
-    TRY(vcycle_t<float>(h, mode, smoother));
+    TRY(run_vcycle<float>(h, mode, smoother));
     k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
     CKL();
     return PGMG_OK;
@@ -433,6 +552,15 @@ pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
         return PGMG_ERR_CUDA;
     }
     h->stream = h->own;
+    for (int size : {16, 8}) {
+        if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0) {
+            h->cluster_size = size;
+            break;
+        }
+    }
+    h->coarse_first = h->nl - 1;
+    for (int l = 0; l < h->nl; l++)
+        if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
     if (cudaMemsetAsync(h->arena.base, 0, bytes, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         pgmg_dev_destroy(h);
@@ -445,6 +573,7 @@ pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
 pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
     if (h->arena.base) cudaFree(h->arena.base);
     if (h->norm_host) cudaFreeHost(h->norm_host);
     if (h->own) cudaStreamDestroy(h->own);
@@ -470,6 +599,39 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle* h, long long* n) {
     if (!h || !n) return PGMG_ERR_ARG;
     *n = h->launches;
     return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
+    if (!h) return PGMG_ERR_ARG;
+    switch (key) {
+        case PGMG_OPT_GRAPHS:
+            drop_graphs(h);
+            h->use_graphs = value != 0;
+            return PGMG_OK;
+        case PGMG_OPT_CLUSTER_FIRST:
+            if (value < 0 || value > h->nl) return fail(h, PGMG_ERR_ARG, "cluster level %lld out of range", value);
+            drop_graphs(h);
+            h->coarse_first = (int)value;
+            return PGMG_OK;
+        case PGMG_OPT_CLUSTER_SIZE:
+            if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
+            if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
+                return fail(h, PGMG_ERR_UNSUPPORTED, "cluster of %lld CTAs not launchable", value);
+            drop_graphs(h);
+            h->cluster_size = (int)value;
+            return PGMG_OK;
+    }
+    return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
+}
+
+pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
+    if (!h || !value) return PGMG_ERR_ARG;
+    switch (key) {
+        case PGMG_OPT_GRAPHS: *value = h->use_graphs; return PGMG_OK;
+        case PGMG_OPT_CLUSTER_FIRST: *value = h->coarse_first; return PGMG_OK;
+        case PGMG_OPT_CLUSTER_SIZE: *value = h->cluster_size; return PGMG_OK;
+    }
+    return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
 
 pgmg_status pgmg_dev_set_smoother(pgmg_handle* h, int smoother) {
@@ -556,6 +718,7 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
 pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->uploaded) return fail(h, PGMG_ERR_SETUP, "level-0 stencils not uploaded");
+    drop_graphs(h);
     for (int l = 1; l < h->nl; l++) {
         Level& F = h->L[l - 1];
         Level& Cl = h->L[l];
@@ -612,6 +775,7 @@ pgmg_status pgmg_dev_get_boxes(pgmg_handle* h, int level, int* S6) {
 
 pgmg_status pgmg_dev_set_field(pgmg_handle* h, int level, int field, const double* src) {
     TRY(check_level(h, level));
+    if (field == PGMG_FIELD_X) h->x0_zero = false;
     if (!src || (field != PGMG_FIELD_X && field != PGMG_FIELD_R)) return PGMG_ERR_ARG;
     Level& L = h->L[level];
     const LevelGeom& g = L.g;
@@ -642,6 +806,7 @@ pgmg_status pgmg_dev_get_field(pgmg_handle* h, int level, int field, double* dst
 
 pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
+    if (level == 0) h->x0_zero = true;
     k_clear_x<double><<<nblk(h->L[level].g.npts), kBlock, 0, h->stream>>>(h->L[level].g, h->L[level].x64);
     CKL();
     return PGMG_OK;
@@ -649,6 +814,7 @@ pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
 
 pgmg_status pgmg_dev_setup_test(pgmg_handle* h, int level, int ca, int xfield) {
     TRY(check_level(h, level));
+    h->x0_zero = false;
     Level& L = h->L[level];
     k_setup_test<double><<<nblk(L.g.npts), kBlock, 0, h->stream>>>(L.g, L.x64, L.r64, ca, xfield);
     CKL();
@@ -657,6 +823,7 @@ pgmg_status pgmg_dev_setup_test(pgmg_handle* h, int level, int ca, int xfield) {
 
 pgmg_status pgmg_dev_gs(pgmg_handle* h, int level, int mode, int smoother) {
     TRY(check_level(h, level));
+    h->x0_zero = false;
     if (smoother < 0) smoother = h->dims.smoother;
     return gs_level<double>(h, level, mode, smoother, 1);
 }
@@ -669,6 +836,7 @@ pgmg_status pgmg_dev_restrict(pgmg_handle* h, int level) {
 
 pgmg_status pgmg_dev_interp(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
+    h->x0_zero = false;
     if (level < 1) return fail(h, PGMG_ERR_ARG, "interpolation needs level >= 1");
     return interp_level<double>(h, level);
 }
@@ -676,21 +844,24 @@ pgmg_status pgmg_dev_interp(pgmg_handle* h, int level) {
 pgmg_status pgmg_dev_coarse_solve(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
-    return coarse_solve_t<double>(h);
+    if (h->nl == 1) h->x0_zero = false;
+    return coarse_solve_t<double>(h, h->dims.smoother);
 }
 
 pgmg_status pgmg_dev_vcycle(pgmg_handle* h, int mode, int smoother) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (smoother < 0) smoother = h->dims.smoother;
+    h->x0_zero = false;
     if (h->dims.precision == PGMG_MIXED) return ir_step(h, mode, smoother, nullptr, nullptr);
-    return vcycle_t<double>(h, mode, smoother);
+    return run_vcycle<double>(h, mode, smoother);
 }
 
 pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (smoother < 0) smoother = h->dims.smoother;
+    h->x0_zero = false;
     // multigrid::fmg_cycle (multigrid.cc:109-134), v_down = v_up = 2,
     // v_bottom = 20 (multigrid.hh:284), mode 0.
     int ml = h->nl;
@@ -763,15 +934,24 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result,
 // converged solve rarely pays for more than one check past the prediction.
 struct CheckPlan {
     int every;
+    double rho0 = 0;  // reduction factor remembered from an earlier solve
     int last_n = -1, prev_n = -1;
     double last_r = 0, prev_r = 0;
+    double rho() const {
+        if (prev_n >= 0 && last_r > 0 && prev_r > 0) return pow(last_r / prev_r, 1.0 / (last_n - prev_n));
+        return rho0;
+    }
     int next(int nc, double tol) const {
         if (every >= 1) return nc + every;
-        if (prev_n < 0 || last_r <= 0 || prev_r <= 0) return nc + 1;
-        double rho = pow(last_r / prev_r, 1.0 / (last_n - prev_n));
-        if (!(rho > 0) || rho >= 0.9) return nc + 1;
-        int need = (int)ceil(log(tol / last_r) / log(rho));
-        return nc + (need > 2 ? need - 1 : 1);
+        double q = rho();
+        if (!(q > 0) || q >= 0.9 || !(last_r > 0)) return nc + 1;
+        double need = log(tol / last_r) / log(q);
+        int n = (int)ceil(need);
+        if (n < 1) n = 1;
+        // Run the predicted count only when it lands well below tol;
+        // otherwise stop one cycle short and check again.
+        bool margin = last_r * pow(q, n) < 0.3 * tol;
+        return nc + (margin || n == 1 ? n : n - 1);
     }
     void record(int nc, double r) { prev_n = last_n; prev_r = last_r; last_n = nc; last_r = r; }
 };
@@ -791,9 +971,16 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
     dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
     bool mixed = h->dims.precision == PGMG_MIXED;
+    plan.rho0 = h->last_rho;
     for (;;) {
         bool check = nc >= next_check || nc >= max_cycles;
-        if (mixed) {
+        bool zero = nc == 0 && h->x0_zero;  // residual = source: no stencil pass needed
+        if (zero) {
+            if (mixed || check) {
+                k_source<double, float><<<grid, kBlock, 0, h->stream>>>(g, L0.r64, mixed ? L0.r32 : nullptr, h->partials);
+                CKL();
+            }
+        } else if (mixed) {
             // FP64 residual of the current x, stored FP32 as the correction's
             // source (and reduced to the norms when checking).
             k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32,
@@ -817,16 +1004,25 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             next_check = plan.next(nc, tol);
             if (next_check > max_cycles) next_check = max_cycles;
         }
+        h->x0_zero = false;
         if (mixed) {
             k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
             CKL();
-            TRY(vcycle_t<float>(h, 0, smoother));
+            TRY(run_vcycle<float>(h, 0, smoother));
             k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
             CKL();
         } else {
-            TRY(vcycle_t<double>(h, 0, smoother));
+            TRY(run_vcycle<double>(h, 0, smoother));
         }
         nc++;
+    }
+    if (plan.prev_n >= 0 && plan.last_n > plan.prev_n) {
+        double q = plan.rho();
+        if (q > 0 && q < 0.9) h->last_rho = q;
+    }
+    if (nc > 0 && rr < tol && plan.last_n >= 0 && nc > plan.last_n && plan.last_r > 0) {
+        double q = pow(rr / plan.last_r, 1.0 / (nc - plan.last_n));
+        if (q > 0 && q < 0.9) h->last_rho = q;
     }
     if (cycles) *cycles = nc;
     if (relres) *relres = rr;

@@ -1,0 +1,239 @@
+// The coarse tail of the V-cycle in one thread-block cluster.
+//
+// Levels below a few tens of thousands of points are latency-bound: one
+// colour pass of a 17^3 level is a few microseconds of launch and drain for
+// a megabyte of data.  This kernel runs every level from `first` down to the
+// bottom and back up -- 8-colour sweeps, residual restriction, the bottom
+// solve, interpolation -- inside a single cluster of CTAs on neighbouring SMs,
+// separating dependent phases with hardware cluster barriers
+// (barrier.cluster.arrive.release / wait.acquire) instead of kernel launches.
+// The barriers are the hardware's; there are no software spin-waits.
+//
+// Data written by one phase and read by another CTA in a later phase (x, r,
+// the residual scratch) is loaded with ld.global.cg (L2, never a stale L1
+// line); read-only stencils and the coarse inverse go through the normal
+// path.  The arithmetic is the same as the grid kernels' (reference-order,
+// no fused multiply-add), so the cluster path gives bit-identical results.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "layout.cuh"
+
+namespace pgmg {
+
+constexpr int kMaxLv = 16;
+
+template <class T>
+struct CoarsePlan {
+    int first, nl;       // levels first..nl-1 run here
+    int lu_ok;           // bottom: 1 = explicit-inverse solve, 0 = 24 sweeps
+    LevelGeom g[kMaxLv];
+    const T* A[kMaxLv];
+    T* x[kMaxLv];
+    T* r[kMaxLv];
+    T* res[kMaxLv];
+    const double* Minv;
+};
+
+__device__ __forceinline__ void cluster_sync() { cooperative_groups::this_cluster().sync(); }
+
+template <class T>
+__device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, const T* A, int col, int tid, int nth) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    for (long p = tid; p < nc; p += nth) {
+        int i2 = (int)(p % g.M2);
+        long t = p / g.M2;
+        int j2 = (int)(t % g.N2);
+        int k2 = (int)(t / g.N2);
+        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+        if (i >= g.m || j >= g.n || k >= g.o) continue;
+        long xc = g.xi(i, j, k);
+        const T* Ap = A + (long)col * 27 * g.Nc + p;
+        T acc = T(0);
+#pragma unroll
+        for (int q = 0; q < 27; q++) {
+            if (q == 13) continue;
+            acc = madd<true, T>(acc, __ldg(Ap + q * g.Nc), __ldcg(x + xc + slot_off(g, q)));
+        }
+        T inv = T(1) / __ldg(Ap + 13 * g.Nc);
+        x[xc] = mul_rn<T>(sub_rn<T>(__ldcg(r + (long)col * g.Nc + p), acc), inv);
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void c_sweeps(const LevelGeom& g, T* x, const T* r, const T* A, int sweeps, int mode,
+                                         int tid, int nth) {
+    for (int s = 0; s < sweeps; s++)
+        for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+            for (int cc = 0; cc < 8; cc++) {
+                c_colour<T>(g, x, r, A, pass ? 7 - cc : cc, tid, nth);
+                cluster_sync();
+            }
+}
+
+template <class T>
+__device__ __forceinline__ void c_residual(const LevelGeom& g, const T* x, const T* r, const T* A, T* res, int tid,
+                                           int nth) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    for (long pp = tid; pp < 8 * nc; pp += nth) {
+        int col = (int)(pp / nc);
+        long p = pp % nc;
+        int i2 = (int)(p % g.M2);
+        long t = p / g.M2;
+        int j2 = (int)(t % g.N2);
+        int k2 = (int)(t / g.N2);
+        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+        if (i >= g.m || j >= g.n || k >= g.o) continue;
+        long xc = g.xi(i, j, k);
+        const T* Ap = A + (long)col * 27 * g.Nc + p;
+        T acc = T(0);
+#pragma unroll
+        for (int q = 0; q < 27; q++) acc = madd<true, T>(acc, __ldg(Ap + q * g.Nc), __ldcg(x + xc + slot_off(g, q)));
+        res[(long)col * g.Nc + p] = sub_rn<T>(__ldcg(r + (long)col * g.Nc + p), acc);
+    }
+}
+
+// Same accumulation order as k_restrict (reference restriction order).
+template <class T>
+__device__ __forceinline__ void c_restrict(const LevelGeom& gf, const LevelGeom& gc, const T* res, T* rc, T* xc,
+                                           int tid, int nth) {
+    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    for (long q = tid; q < gc.npts; q += nth) {
+        int I = (int)(q % gc.m);
+        long t = q / gc.m;
+        int J = (int)(t % gc.n);
+        int K = (int)(t / gc.n);
+        T acc = T(0);
+        for (int cz = K - 1; cz <= K; cz++) {
+            if (cz < 0 || cz > lz) continue;
+            bool zsn = snapped(cz, gf.o);
+            for (int cy = J - 1; cy <= J; cy++) {
+                if (cy < 0 || cy > ly) continue;
+                for (int cx = I - 1; cx <= I; cx++) {
+                    if (cx < 0 || cx > lx) continue;
+                    bool xsn = snapped(cx, gf.m);
+                    for (int dz = 0; dz < 2; dz++) {
+                        if (dz && !has_upper(cz, gf.o)) continue;
+                        double wz = tweight(cz, dz, K, zsn);
+                        if (wz == 0.0) continue;
+                        for (int dy = 0; dy < 2; dy++) {
+                            if (dy && !has_upper(cy, gf.n)) continue;
+                            for (int dx = 0; dx < 2; dx++) {
+                                if (dx && !has_upper(cx, gf.m)) continue;
+                                bool ysn = (!dx && dy && dz) ? xsn : snapped(cy, gf.n);
+                                double w = tweight(cx, dx, I, xsn) * tweight(cy, dy, J, ysn) * wz;
+                                if (w == 0.0) continue;
+                                T rd = (T)(0.125 * w) * __ldcg(res + gf.ri(2 * cx + dx, 2 * cy + dy, 2 * cz + dz));
+                                acc = add_rn<T>(acc, rd);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        rc[gc.ri(I, J, K)] = acc;
+        xc[gc.xi(I, J, K)] = T(0);
+    }
+}
+
+// Same values as k_interp.
+template <class T>
+__device__ __forceinline__ void c_interp(const LevelGeom& gf, const LevelGeom& gc, T* xf, const T* xcv, int tid,
+                                         int nth) {
+    for (long q = tid; q < gf.npts; q += nth) {
+        int i = (int)(q % gf.m);
+        long t = q / gf.m;
+        int j = (int)(t % gf.n);
+        int k = (int)(t / gf.n);
+        int Cx = i >> 1, Cy = j >> 1, Cz = k >> 1, dx = i & 1, dy = j & 1, dz = k & 1;
+        long b = gc.xi(Cx, Cy, Cz);
+        long sy = gc.mx, sz = gc.mx * gc.my;
+        T v0 = __ldcg(xcv + b), v1 = __ldcg(xcv + b + 1), v2 = __ldcg(xcv + b + sy), v3 = __ldcg(xcv + b + sy + 1);
+        T v4 = __ldcg(xcv + b + sz), v5 = __ldcg(xcv + b + sz + 1), v6 = __ldcg(xcv + b + sz + sy),
+          v7 = __ldcg(xcv + b + sz + sy + 1);
+        const T h = T(0.5), qq = T(0.25), e = T(0.125);
+        int role = dx | (dy << 1) | (dz << 2);
+        T val;
+        bool full = Cx < cube_last(gf.m) && Cy < cube_last(gf.n) && Cz < cube_last(gf.o);
+        if (full) {
+            switch (role) {
+                case 0: val = v0; break;
+                case 1: val = h * (v0 + v1); break;
+                case 2: val = h * (v0 + v2); break;
+                case 3: val = qq * (((v0 + v1) + v2) + v3); break;
+                case 4: val = h * (v0 + v4); break;
+                case 5: val = qq * ((v0 + v1) + (v4 + v5)); break;
+                case 6: val = qq * (((v0 + v2) + v4) + v6); break;
+                default: val = e * (((((((v0 + v1) + v2) + v3) + (v4 + v5)) + v6) + v7)); break;
+            }
+        } else {
+            bool xs = snapped(Cx, gf.m), ys = snapped(Cy, gf.n), zs = snapped(Cz, gf.o);
+            switch (role) {
+                case 0: val = v0; break;
+                case 1: val = xs ? v1 : h * (v0 + v1); break;
+                case 2: val = ys ? v2 : h * (v0 + v2); break;
+                case 4: val = zs ? v4 : h * (v0 + v4); break;
+                case 5: val = zs ? (xs ? v5 : h * (v4 + v5)) : (xs ? h * (v1 + v5) : qq * (((v0 + v1) + v4) + v5)); break;
+                case 6: val = zs ? (ys ? v6 : h * (v4 + v6)) : (ys ? h * (v2 + v6) : qq * (((v0 + v2) + v4) + v6)); break;
+                default: {
+                    T t2 = ys ? (xs ? v3 : h * (v2 + v3)) : (xs ? h * (v1 + v3) : qq * (((v0 + v1) + v2) + v3));
+                    if (role == 3) { val = t2; break; }
+                    T t3 = ys ? (xs ? v7 : h * (v6 + v7)) : (xs ? h * (v5 + v7) : qq * (((v4 + v5) + v6) + v7));
+                    val = zs ? t3 : h * (t3 + t2);
+                }
+            }
+        }
+        long xf_i = gf.xi(i, j, k);
+        xf[xf_i] = __ldcg(xf + xf_i) + val;
+    }
+}
+
+// x = Minv r on the bottom level, one warp per row (same reduction as k_lu_apply).
+template <class T>
+__device__ __forceinline__ void c_lu_apply(const LevelGeom& g, const double* Minv, const T* r, T* x, int tid, int nth) {
+    int n = (int)g.npts;
+    int lane = tid & 31;
+    for (int row = tid >> 5; row < n; row += nth >> 5) {
+        double s = 0.0;
+        for (int c = lane; c < n; c += 32) {
+            int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+            s = fma(Minv[(long)row * n + c], (double)__ldcg(r + g.ri(i, j, k)), s);
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            int i = row % g.m, t = row / g.m, j = t % g.n, k = t / g.n;
+            x[g.xi(i, j, k)] = (T)s;
+        }
+    }
+}
+
+// The V-cycle from level `first` (its source already restricted) to the
+// bottom and back, 8-colour smoothing: 2+l pre- and post-sweeps on level l
+// (multigrid.cc:88-106).  blockDim.x must be a multiple of 32.
+template <class T>
+__global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode) {
+    int nth = gridDim.x * blockDim.x;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int nl = P.nl;
+    for (int l = P.first; l < nl - 1; l++) {
+        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], 2 + l, mode, tid, nth);
+        c_residual<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.res[l], tid, nth);
+        cluster_sync();
+        c_restrict<T>(P.g[l], P.g[l + 1], P.res[l], P.r[l + 1], P.x[l + 1], tid, nth);
+        cluster_sync();
+    }
+    int lb = nl - 1;
+    if (P.lu_ok) {
+        c_lu_apply<T>(P.g[lb], P.Minv, P.r[lb], P.x[lb], tid, nth);
+        cluster_sync();
+    } else {
+        c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, tid, nth);
+    }
+    for (int l = lb; l > P.first; l--) {
+        c_interp<T>(P.g[l - 1], P.g[l], P.x[l - 1], P.x[l], tid, nth);
+        cluster_sync();
+        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], 2 + l - 1, mode, tid, nth);
+    }
+}
+
+}  // namespace pgmg

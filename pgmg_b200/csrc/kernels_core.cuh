@@ -16,14 +16,15 @@ constexpr int kBlock = 256;
 // are zero, so summing all 26 in slot order is the reference's box order.
 template <class T, bool EXACT>
 __device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ x, long xc,
-                                      const T* __restrict__ Ap, long plane, T rv) {
+                                      const T* __restrict__ Ap, long plane, T rv, uint64_t pstream,
+                                      uint64_t pkeep) {
     T acc = T(0);
 #pragma unroll
     for (int q = 0; q < 27; q++) {
         if (q == 13) continue;
-        acc = madd<EXACT, T>(acc, __ldg(Ap + q * plane), __ldg(x + xc + slot_off(g, q)));
+        acc = madd<EXACT, T>(acc, ld_stream(Ap + q * plane, pstream), ld_keep(x + xc + slot_off(g, q), pkeep));
     }
-    T inv = T(1) / __ldg(Ap + 13 * plane);
+    T inv = T(1) / ld_stream(Ap + 13 * plane, pstream);
     if (EXACT) return mul_rn<T>(sub_rn<T>(rv, acc), inv);
     return (rv - acc) * inv;
 }
@@ -45,9 +46,11 @@ __global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T
     int k2 = (int)(t / g.N2);
     int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
     if (i >= g.m || j >= g.n || k >= g.o) return;
+    uint64_t ps = policy_evict_first(), pk = policy_evict_last();
     long xc = g.xi(i, j, k);
     const T* Ap = A + (long)col * 27 * g.Nc + p;
-    x[xc] = gs_value<T, EXACT>(g, x, xc, Ap, g.Nc, __ldg(r + (long)col * g.Nc + p));
+    T v = gs_value<T, EXACT>(g, x, xc, Ap, g.Nc, ld_stream(r + (long)col * g.Nc + p, ps), ps, pk);
+    st_keep(x + xc, v, pk);
 }
 
 // Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of
@@ -216,12 +219,14 @@ __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __res
         int k2 = (int)(t / g.N2);
         int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
         if (i < g.m && j < g.n && k < g.o) {
+            uint64_t ps = policy_evict_first(), pk = policy_evict_last();
             long xc = g.xi(i, j, k);
             const T* Ap = A + (long)col * 27 * g.Nc + p;
             T acc = T(0);
 #pragma unroll
-            for (int q = 0; q < 27; q++) acc = madd<EXACT, T>(acc, __ldg(Ap + q * g.Nc), __ldg(x + xc + slot_off(g, q)));
-            T rv = __ldg(r + (long)col * g.Nc + p);
+            for (int q = 0; q < 27; q++)
+                acc = madd<EXACT, T>(acc, ld_stream(Ap + q * g.Nc, ps), ld_keep(x + xc + slot_off(g, q), pk));
+            T rv = ld_stream(r + (long)col * g.Nc + p, ps);
             T res = EXACT ? sub_rn<T>(rv, acc) : rv - acc;
             if (out) out[(long)col * g.Nc + p] = (TO)res;
             s_res = (double)res * (double)res;
@@ -235,6 +240,31 @@ __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __res
             partials[2 * b] = s_res;
             partials[2 * b + 1] = s_rhs;
         }
+    }
+}
+
+// Sum of squared sources of a level (res^2 = r^2 when x = 0), optionally
+// copying the source to `out` (the FP32 correction source of mixed
+// precision).  Same grid and partials layout as k_residual.
+template <class T, class TO>
+__global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restrict__ r, TO* __restrict__ out,
+                                                   double* __restrict__ partials) {
+    __shared__ double sh[64];
+    int col = blockIdx.y;
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    double s = 0;
+    if (p < nc) {
+        T rv = r[(long)col * g.Nc + p];
+        if (out) out[(long)col * g.Nc + p] = (TO)rv;
+        s = (double)rv * (double)rv;
+    }
+    double s2 = s;
+    block_sum2(s, s2, sh);
+    if (threadIdx.x == 0) {
+        long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
+        partials[2 * b] = s;
+        partials[2 * b + 1] = s2;
     }
 }
 

@@ -118,6 +118,47 @@ template <bool EXACT, class T> __device__ inline T madd(T acc, T a, T b) {
     return fma(a, b, acc);
 }
 
+// L2 eviction-priority hints.  Stencil coefficients and sources are
+// streamed once per pass (evict_first, and not kept in L1); the solution
+// vector is re-read by every colour pass and by the residual, so it is loaded
+// and stored with evict_last to keep as much of it in L2 as fits.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_stream(const double* a, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float* a, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_keep(const double* a, uint64_t pol) {
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float* a, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_keep(double* a, double v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+
 // Offset of slot q in the halo'd x array.
 __host__ __device__ inline long slot_off(const LevelGeom& g, int q) {
     int di = q % 3 - 1, dj = (q / 3) % 3 - 1, dk = q / 9 - 1;

@@ -235,3 +235,31 @@ def test_errors_are_statuses():
     assert e.value.status == 7
     with pytest.raises(P.PgmgError):
         G.gauss_seidel(0, 5)
+
+
+@pytest.mark.parametrize("mno", [(33, 33, 33), (65, 65, 65), (41, 41, 41), (16, 17, 18), (20, 33, 9)])
+def test_mc8_vcycle_bitwise(mno):
+    """The 8-colour V-cycle (grid kernels on fine levels, the one-cluster
+    kernel on coarse ones, 24 coarse sweeps) equals the oracle's 8-colour
+    V-cycle bit for bit."""
+    G, prob = make(mno, coarse=P.COARSE_GS, smoother=P.SMOOTH_MC8)
+    O = oracle_for(mno, prob, False)
+    O.set_smoother(True)
+    for it in range(3):
+        G.v_cycle(0)
+        O.v_cycle(0)
+        assert np.array_equal(G.get_x(0), O.get_x(0)), f"cycle {it}"
+    G.v_cycle(1)
+    O.v_cycle(1)
+    assert np.array_equal(G.get_x(0), O.get_x(0))
+
+
+@pytest.mark.parametrize("mno", [(33, 33, 33), (65, 65, 65)])
+def test_mc8_vcycle_with_lu_close(mno):
+    G, prob = make(mno, coarse=P.COARSE_LU, smoother=P.SMOOTH_MC8)
+    O = oracle_for(mno, prob, True)
+    O.set_smoother(True)
+    for it in range(3):
+        G.v_cycle(0)
+        O.v_cycle(0)
+        assert relerr(G.get_x(0), O.get_x(0)) < 1e-12, f"cycle {it}"
