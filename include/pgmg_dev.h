@@ -120,13 +120,17 @@ pgmg_status pgmg_dev_sync(pgmg_handle *h);
 const char *pgmg_dev_last_error(pgmg_handle *h);
 /* Kernels the handle has launched so far (all of them this library's own). */
 pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
-/* Execution options (tuning; results do not depend on them).
+/* Execution options (tuning; results do not depend on them unless noted).
  *   PGMG_OPT_GRAPHS         1 = replay each V-cycle as a captured CUDA graph (default)
  *   PGMG_OPT_CLUSTER_FIRST  first level run by the one-cluster coarse cycle
  *                           (default: the first level of <= 50000 points;
  *                           = number of levels disables it)
- *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 16, 8, or 0 (off) */
-enum { PGMG_OPT_GRAPHS = 1, PGMG_OPT_CLUSTER_FIRST = 2, PGMG_OPT_CLUSTER_SIZE = 3 };
+ *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 16, 8, or 0 (off)
+ *   PGMG_OPT_SLAB_BUDGET    bytes of solution vector per z-slab of the 8-colour
+ *                           sweep (default 0 = one slab).  This one
+ *                           changes the update order, so results change at
+ *                           rounding level and convergence slightly. */
+enum { PGMG_OPT_GRAPHS = 1, PGMG_OPT_CLUSTER_FIRST = 2, PGMG_OPT_CLUSTER_SIZE = 3, PGMG_OPT_SLAB_BUDGET = 4 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
 /* Default smoother of pgmg_dev_vcycle and the solves. */

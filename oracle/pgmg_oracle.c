@@ -48,6 +48,7 @@ struct orc {
 	double iter_avg,iter_var,alpha,tol;
 	int v_down,v_up,v_bottom;
 	int smoother;  /* 0 = lexicographic (reference), 1 = 8-colour */
+	long long slab_budget;  /* bytes of FP64 x per z-slab of the 8-colour sweep */
 };
 
 static inline long xi(const olev *L,int i,int j,int k) {
@@ -290,6 +291,7 @@ orc* orc_create(int m,int n,int o,const int *S6,const double *c27,const double *
 	orc *h=calloc(1,sizeof(orc));
 	/* multigrid ctor defaults, multigrid.hh:283-285 */
 	h->v_down=2;h->v_bottom=20;h->v_up=2;
+	h->slab_budget=0;
 	/* mg_guide(), multigrid.hh:79-82, set_period :107-111 */
 	h->period=16;h->iter=16;h->iter_avg=16;h->iter_var=1000000;h->alpha=3.0/16;
 	level_alloc(&h->L[0],m,n,o);
@@ -353,13 +355,33 @@ void orc_gauss_seidel(orc *h,int mode,int l) {
 void orc_gauss_seidel_mc8(orc *h,int mode,int l) {
 	olev *L=&h->L[l];
 	h->gs_num++;
+	/* Slab blocking: a level whose FP64 solution array (with its one-point
+	 * halo) exceeds slab_budget bytes is swept in z-slabs of colour planes,
+	 * all 8 colours of a slab before the next; slab s covers colour planes
+	 * k2 in [O2*s/S, O2*(s+1)/S). */
+	int O2=(L->o+1)/2,S=1;
+	long long xb=(long long)(L->m+2)*(L->n+2)*(L->o+2)*8;
+	if(h->slab_budget>0&&xb>h->slab_budget) {
+		long long q=(xb+h->slab_budget-1)/h->slab_budget;
+		S=(int)(q<O2?q:O2);
+	}
 	for(int pass=0;pass<(mode?2:1);pass++)
-	for(int cc=0;cc<8;cc++) {
-		int c=pass?7-cc:cc;
-		int a=c&1,b=(c>>1)&1,e=(c>>2)&1;
-		for(int k=e;k<L->o;k+=2) for(int j=b;j<L->n;j+=2) for(int i=a;i<L->m;i+=2) gs_point(L,i,j,k);
+	for(int ss=0;ss<S;ss++) {
+		int sl=pass?S-1-ss:ss;
+		int k2lo=(int)((long long)O2*sl/S),k2hi=(int)((long long)O2*(sl+1)/S);
+		for(int cc=0;cc<8;cc++) {
+			int c=pass?7-cc:cc;
+			int a=c&1,b=(c>>1)&1,e=(c>>2)&1;
+			for(int k2=k2lo;k2<k2hi;k2++) {
+				int k=2*k2+e;
+				if(k>=L->o) continue;
+				for(int j=b;j<L->n;j+=2) for(int i=a;i<L->m;i+=2) gs_point(L,i,j,k);
+			}
+		}
 	}
 }
+
+void orc_set_slab_budget(orc *h,long long bytes) {h->slab_budget=bytes;}
 
 /* region::restriction (region.cc:546-572) with restrict_full/partial
  * (:818-912): clear the coarse r, then for each fine point in cube scan

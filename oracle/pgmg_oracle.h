@@ -39,6 +39,9 @@ void orc_gauss_seidel_mc8(orc *h,int mode,int l);
 /* Smoother of orc_v_cycle and of the coarse fallback sweeps: 0 = the
  * reference's lexicographic Gauss-Seidel (default), 1 = 8-colour. */
 void orc_set_smoother(orc *h,int mc8);
+/* Slab budget of the 8-colour sweep in bytes of FP64 solution vector
+ * (default 0 = one slab, the library's default). */
+void orc_set_slab_budget(orc *h,long long bytes);
 void orc_restriction(orc *h,int l);
 void orc_interpolation(orc *h,int l);
 void orc_solve_exact(orc *h,int l);

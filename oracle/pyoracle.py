@@ -176,6 +176,8 @@ def oracle_lib():
         lib.orc_get_A27.argtypes = [C.c_void_p, C.c_int, _dp]
         lib.orc_gauss_seidel_mc8.restype = None
         lib.orc_gauss_seidel_mc8.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        lib.orc_set_slab_budget.restype = None
+        lib.orc_set_slab_budget.argtypes = [C.c_void_p, C.c_longlong]
         lib.orc_set_smoother.restype = None
         lib.orc_set_smoother.argtypes = [C.c_void_p, C.c_int]
         lib.orc_dgetrf.restype = C.c_int
@@ -234,6 +236,9 @@ class Oracle(_Base):
 
     def set_smoother(self, mc8: bool):
         self.lib.orc_set_smoother(self.h, int(mc8))
+
+    def set_slab_budget(self, nbytes: int):
+        self.lib.orc_set_slab_budget(self.h, int(nbytes))
 
 
 class Reference(_Base):

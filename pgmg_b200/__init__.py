@@ -25,7 +25,7 @@ FP64, MIXED = 0, 1
 SMOOTH_MC8, SMOOTH_LEX = 0, 1
 COARSE_LU, COARSE_GS, COARSE_LU_EXACT = 0, 1, 2
 FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
-OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE = 1, 2, 3
+OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE, OPT_SLAB_BUDGET = 1, 2, 3, 4
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",

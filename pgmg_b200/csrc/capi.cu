@@ -85,6 +85,7 @@ struct pgmg_handle {
     // first level it handles.
     int cluster_size = 0;
     int coarse_first = 0;
+    long long slab_budget = 0;  // bytes of x per slab of the 8-colour sweep (0 = one slab)
     char err[512] = {0};
 };
 
@@ -211,17 +212,22 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         return PGMG_OK;
     }
     if (g.npts <= kMc8BlockMax) {
-        k_gs_mc8_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode);
+        k_gs_mc8_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode, h->slab_budget);
         CKL();
         return PGMG_OK;
     }
-    long nc = (long)g.M2 * g.N2 * g.O2;
+    int S = slab_count(g, (int)sizeof(T), h->slab_budget);
     for (int s = 0; s < sweeps; s++)
         for (int pass = 0; pass < (mode ? 2 : 1); pass++)
-            for (int cc = 0; cc < 8; cc++) {
-                int col = pass ? 7 - cc : cc;
-                k_gs_colour<T, true><<<nblk(nc), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, col);
-                CKL();
+            for (int ss = 0; ss < S; ss++) {
+                int sl = pass ? S - 1 - ss : ss;
+                int k2lo = slab_lo(g, sl, S), k2hi = slab_lo(g, sl + 1, S);
+                long np = (long)(k2hi - k2lo) * g.M2 * g.N2;
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = pass ? 7 - cc : cc;
+                    k_gs_colour<T, true><<<nblk(np), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, col, k2lo, k2hi);
+                    CKL();
+                }
             }
     return PGMG_OK;
 }
@@ -284,6 +290,7 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     P.first = first;
     P.nl = h->nl;
     P.lu_ok = h->lu_ok;
+    P.slab_budget = h->slab_budget;
     P.Minv = h->Minv;
     for (int l = 0; l < h->nl; l++) {
         View<T> v = view<T>(h->L[l]);
@@ -613,6 +620,10 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             drop_graphs(h);
             h->coarse_first = (int)value;
             return PGMG_OK;
+        case PGMG_OPT_SLAB_BUDGET:
+            drop_graphs(h);
+            h->slab_budget = value;
+            return PGMG_OK;
         case PGMG_OPT_CLUSTER_SIZE:
             if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
             if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
@@ -630,6 +641,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_GRAPHS: *value = h->use_graphs; return PGMG_OK;
         case PGMG_OPT_CLUSTER_FIRST: *value = h->coarse_first; return PGMG_OK;
         case PGMG_OPT_CLUSTER_SIZE: *value = h->cluster_size; return PGMG_OK;
+        case PGMG_OPT_SLAB_BUDGET: *value = h->slab_budget; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }

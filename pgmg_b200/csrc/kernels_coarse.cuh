@@ -27,6 +27,7 @@ template <class T>
 struct CoarsePlan {
     int first, nl;       // levels first..nl-1 run here
     int lu_ok;           // bottom: 1 = explicit-inverse solve, 0 = 24 sweeps
+    long long slab_budget;  // slab order of the 8-colour sweeps (as the grid path)
     LevelGeom g[kMaxLv];
     const T* A[kMaxLv];
     T* x[kMaxLv];
@@ -38,9 +39,9 @@ struct CoarsePlan {
 __device__ __forceinline__ void cluster_sync() { cooperative_groups::this_cluster().sync(); }
 
 template <class T>
-__device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, const T* A, int col, int tid, int nth) {
-    long nc = (long)g.M2 * g.N2 * g.O2;
-    for (long p = tid; p < nc; p += nth) {
+__device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, const T* A, int col, long p0, long p1,
+                                         int tid, int nth) {
+    for (long p = p0 + tid; p < p1; p += nth) {
         int i2 = (int)(p % g.M2);
         long t = p / g.M2;
         int j2 = (int)(t % g.N2);
@@ -62,12 +63,17 @@ __device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, c
 
 template <class T>
 __device__ __forceinline__ void c_sweeps(const LevelGeom& g, T* x, const T* r, const T* A, int sweeps, int mode,
-                                         int tid, int nth) {
+                                         long long budget, int tid, int nth) {
+    int S = slab_count(g, (int)sizeof(T), budget);
     for (int s = 0; s < sweeps; s++)
         for (int pass = 0; pass < (mode ? 2 : 1); pass++)
-            for (int cc = 0; cc < 8; cc++) {
-                c_colour<T>(g, x, r, A, pass ? 7 - cc : cc, tid, nth);
-                cluster_sync();
+            for (int ss = 0; ss < S; ss++) {
+                int sl = pass ? S - 1 - ss : ss;
+                long p0 = (long)slab_lo(g, sl, S) * g.M2 * g.N2, p1 = (long)slab_lo(g, sl + 1, S) * g.M2 * g.N2;
+                for (int cc = 0; cc < 8; cc++) {
+                    c_colour<T>(g, x, r, A, pass ? 7 - cc : cc, p0, p1, tid, nth);
+                    cluster_sync();
+                }
             }
 }
 
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode)
     int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int nl = P.nl;
     for (int l = P.first; l < nl - 1; l++) {
-        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], 2 + l, mode, tid, nth);
+        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], 2 + l, mode, P.slab_budget, tid, nth);
         c_residual<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.res[l], tid, nth);
         cluster_sync();
         c_restrict<T>(P.g[l], P.g[l + 1], P.res[l], P.r[l + 1], P.x[l + 1], tid, nth);
@@ -227,12 +233,12 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode)
         c_lu_apply<T>(P.g[lb], P.Minv, P.r[lb], P.x[lb], tid, nth);
         cluster_sync();
     } else {
-        c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, tid, nth);
+        c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, P.slab_budget, tid, nth);
     }
     for (int l = lb; l > P.first; l--) {
         c_interp<T>(P.g[l - 1], P.g[l], P.x[l - 1], P.x[l], tid, nth);
         cluster_sync();
-        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], 2 + l - 1, mode, tid, nth);
+        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], 2 + l - 1, mode, P.slab_budget, tid, nth);
     }
 }
 

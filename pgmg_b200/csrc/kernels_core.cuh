@@ -36,10 +36,9 @@ __device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ 
 // consecutive threads is contiguous (structure-of-arrays per colour).
 template <class T, bool EXACT>
 __global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
-                                                      const T* __restrict__ A, int col) {
-    long nc = (long)g.M2 * g.N2 * g.O2;
-    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (p >= nc) return;
+                                                      const T* __restrict__ A, int col, int k2lo, int k2hi) {
+    long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (p >= (long)k2hi * g.M2 * g.N2) return;
     int i2 = (int)(p % g.M2);
     long t = p / g.M2;
     int j2 = (int)(t % g.N2);
@@ -147,33 +146,39 @@ __global__ void __launch_bounds__(1024) k_gs_lex_block(LevelGeom g, T* x, const 
     }
 }
 
-// 8-colour sweep of a small level in one thread block.
+// 8-colour sweep of a small level in one thread block (slab order as
+// k_gs_colour's launches).
 template <class T>
 __global__ void __launch_bounds__(1024) k_gs_mc8_block(LevelGeom g, T* x, const T* __restrict__ r,
-                                                       const T* __restrict__ A, int sweeps, int mode) {
-    long nc = (long)g.M2 * g.N2 * g.O2;
+                                                       const T* __restrict__ A, int sweeps, int mode,
+                                                       long long slab_budget) {
+    int S = slab_count(g, (int)sizeof(T), slab_budget);
     for (int s = 0; s < sweeps; s++) {
         for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
-            for (int cc = 0; cc < 8; cc++) {
-                int col = pass ? 7 - cc : cc;
-                for (long p = threadIdx.x; p < nc; p += blockDim.x) {
-                    int i2 = (int)(p % g.M2);
-                    long t = p / g.M2;
-                    int j2 = (int)(t % g.N2);
-                    int k2 = (int)(t / g.N2);
-                    int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
-                    if (i >= g.m || j >= g.n || k >= g.o) continue;
-                    long xc = g.xi(i, j, k);
-                    const T* Ap = A + (long)col * 27 * g.Nc + p;
-                    T acc = T(0);
+            for (int ss = 0; ss < S; ss++) {
+                int sl = pass ? S - 1 - ss : ss;
+                long p0 = (long)slab_lo(g, sl, S) * g.M2 * g.N2, p1 = (long)slab_lo(g, sl + 1, S) * g.M2 * g.N2;
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = pass ? 7 - cc : cc;
+                    for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+                        int i2 = (int)(p % g.M2);
+                        long t = p / g.M2;
+                        int j2 = (int)(t % g.N2);
+                        int k2 = (int)(t / g.N2);
+                        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+                        if (i >= g.m || j >= g.n || k >= g.o) continue;
+                        long xc = g.xi(i, j, k);
+                        const T* Ap = A + (long)col * 27 * g.Nc + p;
+                        T acc = T(0);
 #pragma unroll
-                    for (int q = 0; q < 27; q++) {
-                        if (q == 13) continue;
-                        acc = madd<true, T>(acc, Ap[q * g.Nc], x[xc + slot_off(g, q)]);
+                        for (int q = 0; q < 27; q++) {
+                            if (q == 13) continue;
+                            acc = madd<true, T>(acc, Ap[q * g.Nc], x[xc + slot_off(g, q)]);
+                        }
+                        x[xc] = mul_rn<T>(sub_rn<T>(r[(long)col * g.Nc + p], acc), T(1) / Ap[13 * g.Nc]);
                     }
-                    x[xc] = mul_rn<T>(sub_rn<T>(r[(long)col * g.Nc + p], acc), T(1) / Ap[13 * g.Nc]);
+                    __syncthreads();
                 }
-                __syncthreads();
             }
         }
     }

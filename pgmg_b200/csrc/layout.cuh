@@ -65,6 +65,23 @@ inline LevelGeom make_geom(int m, int n, int o) {
     return g;
 }
 
+// Slab blocking of the 8-colour sweep: a level whose solution array exceeds
+// `budget` bytes is swept in `slabs` z-slabs, all 8 colours of slab s before
+// slab s+1 (every ordering of point updates is a Gauss-Seidel sweep; within
+// a slab and colour the points stay independent).  Slab s covers colour
+// sub-grid planes k2 in [O2*s/slabs, O2*(s+1)/slabs).  The rule depends only
+// on the level size, the element size and the budget, so the oracle can
+// reproduce the same order.
+__host__ __device__ inline int slab_count(const LevelGeom& g, int elem_bytes, long long budget) {
+    long long bytes = (long long)g.xsize * elem_bytes;
+    if (budget <= 0 || bytes <= budget) return 1;
+    long long s = (bytes + budget - 1) / budget;
+    return (int)(s < g.O2 ? s : g.O2);
+}
+__host__ __device__ inline int slab_lo(const LevelGeom& g, int s, int slabs) {
+    return (int)((long long)g.O2 * s / slabs);
+}
+
 // Per-axis transfer geometry between a fine axis of size ma and its coarse
 // axis (ma+2)>>1 (region.cc:14), as rt_scan_grid/slice/row walk it on one
 // process (region.cc:665-746): cubes C = 0..last; the lower point 2C always

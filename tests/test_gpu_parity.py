@@ -263,3 +263,21 @@ def test_mc8_vcycle_with_lu_close(mno):
         G.v_cycle(0)
         O.v_cycle(0)
         assert relerr(G.get_x(0), O.get_x(0)) < 1e-12, f"cycle {it}"
+
+
+@pytest.mark.parametrize("mno,budget", [((33, 33, 33), 100_000), ((65, 65, 65), 400_000), ((41, 41, 41), 150_000)])
+def test_mc8_slab_order_bitwise(mno, budget):
+    """Slab-blocked 8-colour sweeps (forced by a small slab budget) on the
+    grid, single-block and cluster paths equal the oracle's slab order."""
+    G, prob = make(mno, coarse=P.COARSE_GS, smoother=P.SMOOTH_MC8)
+    G.set_option(P.OPT_SLAB_BUDGET, budget)
+    O = oracle_for(mno, prob, False)
+    O.set_smoother(True)
+    O.set_slab_budget(budget)
+    for it in range(2):
+        G.v_cycle(0)
+        O.v_cycle(0)
+        assert np.array_equal(G.get_x(0), O.get_x(0)), f"cycle {it}"
+    G.v_cycle(1)
+    O.v_cycle(1)
+    assert np.array_equal(G.get_x(0), O.get_x(0))
