@@ -129,8 +129,20 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *   PGMG_OPT_SLAB_BUDGET    bytes of solution vector per z-slab of the 8-colour
  *                           sweep (default 0 = one slab).  This one
  *                           changes the update order, so results change at
- *                           rounding level and convergence slightly. */
-enum { PGMG_OPT_GRAPHS = 1, PGMG_OPT_CLUSTER_FIRST = 2, PGMG_OPT_CLUSTER_SIZE = 3, PGMG_OPT_SLAB_BUDGET = 4 };
+ *                           rounding level and convergence slightly.
+ *   PGMG_OPT_V_DOWN, PGMG_OPT_V_UP, PGMG_OPT_V_BOTTOM
+ *                           the reference's public sweep counts (multigrid.hh:
+ *                           122-128; defaults 2, 2, 20): level l gets v_down+l
+ *                           pre- and v_up+l-1 post-sweeps (multigrid.cc:92,102). */
+enum {
+    PGMG_OPT_GRAPHS = 1,
+    PGMG_OPT_CLUSTER_FIRST = 2,
+    PGMG_OPT_CLUSTER_SIZE = 3,
+    PGMG_OPT_SLAB_BUDGET = 4,
+    PGMG_OPT_V_DOWN = 5,
+    PGMG_OPT_V_UP = 6,
+    PGMG_OPT_V_BOTTOM = 7
+};
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
 /* Default smoother of pgmg_dev_vcycle and the solves. */
@@ -171,6 +183,9 @@ pgmg_status pgmg_dev_get_boxes(pgmg_handle *h, int level, int *S6);
  * reg[l]->x0 / r0.  PGMG_FIELD_RES is output only. */
 pgmg_status pgmg_dev_set_field(pgmg_handle *h, int level, int field, const double *src);
 pgmg_status pgmg_dev_get_field(pgmg_handle *h, int level, int field, double *dst);
+/* out = A in on a level, natural order, m*n*o doubles each (region::Ax /
+ * mul_A / unpadded_Ax, region.cc:1861-1912; multigrid.hh:226-234). */
+pgmg_status pgmg_dev_apply(pgmg_handle *h, int level, const double *in, double *out);
 /* x = 0 on a level (region::clear_x_field, region.cc:1679-1682). */
 pgmg_status pgmg_dev_clear_x(pgmg_handle *h, int level);
 /* Analytic test fields (region::setup_test, region.cc:1812-1826). */
@@ -192,8 +207,9 @@ pgmg_status pgmg_dev_interp(pgmg_handle *h, int level);
 /* Coarsest-level solve (multigrid::solve_exact, multigrid.hh:265-267;
  * region::solve_exact, region_tr.cc:540-558). */
 pgmg_status pgmg_dev_coarse_solve(pgmg_handle *h);
-/* One V-cycle (multigrid::v_cycle, multigrid.cc:88-106): 2+l pre- and
- * post-sweeps on level l, coarse solve at the bottom.  smoother < 0 uses
+/* One V-cycle (multigrid::v_cycle, multigrid.cc:88-106): v_down+l pre- and
+ * v_up+l-1 post-sweeps on level l (2 and 2 unless set with
+ * pgmg_dev_set_option), coarse solve at the bottom.  smoother < 0 uses
  * the handle's default. */
 pgmg_status pgmg_dev_vcycle(pgmg_handle *h, int mode, int smoother);
 /* Full multigrid cycle (multigrid::fmg_cycle, multigrid.cc:109-134). */

@@ -26,6 +26,7 @@ SMOOTH_MC8, SMOOTH_LEX = 0, 1
 COARSE_LU, COARSE_GS, COARSE_LU_EXACT = 0, 1, 2
 FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
 OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE, OPT_SLAB_BUDGET = 1, 2, 3, 4
+OPT_V_DOWN, OPT_V_UP, OPT_V_BOTTOM = 5, 6, 7
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -77,6 +78,7 @@ SIGNATURES = [
     ("pgmg_dev_get_boxes", C.c_int, [_VP, C.c_int, _VP]),
     ("pgmg_dev_set_field", C.c_int, [_VP, C.c_int, C.c_int, _VP]),
     ("pgmg_dev_get_field", C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    ("pgmg_dev_apply", C.c_int, [_VP, C.c_int, _VP, _VP]),
     ("pgmg_dev_clear_x", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_setup_test", C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
     ("pgmg_dev_gs", C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
@@ -312,6 +314,13 @@ class Multigrid:
 
     def get_residual(self, level=0):
         return self.get_field(level, FIELD_RES)
+
+    def apply(self, level: int, vec) -> np.ndarray:
+        """A @ vec on a level (natural order)."""
+        a = np.ascontiguousarray(vec, np.float64)
+        out = np.empty_like(a)
+        self._ck(lib().pgmg_dev_apply(self._h, level, _ptr(a), _ptr(out)), "apply")
+        return out
 
     def clear_x(self, level=0):
         self._ck(lib().pgmg_dev_clear_x(self._h, level), "clear_x")

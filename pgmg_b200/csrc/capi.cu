@@ -86,6 +86,8 @@ struct pgmg_handle {
     int cluster_size = 0;
     int coarse_first = 0;
     long long slab_budget = 0;  // bytes of x per slab of the 8-colour sweep (0 = one slab)
+    // Public sweep counts of the reference's multigrid (multigrid.hh:122-128).
+    int v_down = 2, v_up = 2, v_bottom = 20;
     char err[512] = {0};
 };
 
@@ -291,6 +293,8 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     P.nl = h->nl;
     P.lu_ok = h->lu_ok;
     P.slab_budget = h->slab_budget;
+    P.v_down = h->v_down;
+    P.v_up = h->v_up;
     P.Minv = h->Minv;
     for (int l = 0; l < h->nl; l++) {
         View<T> v = view<T>(h->L[l]);
@@ -349,14 +353,14 @@ pgmg_status vcycle_t(pgmg_handle* h, int mode, int smoother) {
     int lc = cl ? h->coarse_first : ml;
     int top = lc < ml ? lc : ml - 1;
     for (int i = 0; i < top; i++) {
-        TRY(gs_level<T>(h, i, mode, smoother, 2 + i));
+        TRY(gs_level<T>(h, i, mode, smoother, h->v_down + i));
         TRY(restrict_level<T>(h, i + 1));
     }
     if (lc < ml) TRY(launch_coarse<T>(h, lc, mode));
     else TRY(coarse_solve_t<T>(h, smoother));
     for (int i = top; i > 0; i--) {
         TRY(interp_level<T>(h, i));
-        TRY(gs_level<T>(h, i - 1, mode, smoother, 2 + i - 1));
+        TRY(gs_level<T>(h, i - 1, mode, smoother, h->v_up + i - 1));
     }
     return PGMG_OK;
 }
@@ -624,6 +628,13 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             drop_graphs(h);
             h->slab_budget = value;
             return PGMG_OK;
+        case PGMG_OPT_V_DOWN:
+        case PGMG_OPT_V_UP:
+        case PGMG_OPT_V_BOTTOM:
+            if (value < 0 || value > 1000) return fail(h, PGMG_ERR_ARG, "sweep count %lld out of range", value);
+            drop_graphs(h);
+            (key == PGMG_OPT_V_DOWN ? h->v_down : key == PGMG_OPT_V_UP ? h->v_up : h->v_bottom) = (int)value;
+            return PGMG_OK;
         case PGMG_OPT_CLUSTER_SIZE:
             if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
             if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
@@ -642,6 +653,9 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_CLUSTER_FIRST: *value = h->coarse_first; return PGMG_OK;
         case PGMG_OPT_CLUSTER_SIZE: *value = h->cluster_size; return PGMG_OK;
         case PGMG_OPT_SLAB_BUDGET: *value = h->slab_budget; return PGMG_OK;
+        case PGMG_OPT_V_DOWN: *value = h->v_down; return PGMG_OK;
+        case PGMG_OPT_V_UP: *value = h->v_up; return PGMG_OK;
+        case PGMG_OPT_V_BOTTOM: *value = h->v_bottom; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -816,6 +830,19 @@ pgmg_status pgmg_dev_get_field(pgmg_handle* h, int level, int field, double* dst
     return PGMG_OK;
 }
 
+pgmg_status pgmg_dev_apply(pgmg_handle* h, int level, const double* in, double* out) {
+    TRY(check_level(h, level));
+    if (!in || !out) return PGMG_ERR_ARG;
+    Level& L = h->L[level];
+    const LevelGeom& g = L.g;
+    CK(cudaMemcpyAsync(h->stage, in, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    k_apply<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L.A64, h->stage, L.res64);
+    CKL();
+    CK(cudaMemcpyAsync(out, L.res64, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return PGMG_OK;
+}
+
 pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
     if (level == 0) h->x0_zero = true;
@@ -874,22 +901,21 @@ pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (smoother < 0) smoother = h->dims.smoother;
     h->x0_zero = false;
-    // multigrid::fmg_cycle (multigrid.cc:109-134), v_down = v_up = 2,
-    // v_bottom = 20 (multigrid.hh:284), mode 0.
+    // multigrid::fmg_cycle (multigrid.cc:109-134), mode 0.
     int ml = h->nl;
     for (int i = 0; i < ml - 1; i++) {
         TRY(restrict_level<double>(h, i + 1));
-        TRY(gs_level<double>(h, i + 1, 0, smoother, 2));
+        TRY(gs_level<double>(h, i + 1, 0, smoother, h->v_down));
     }
     for (int j = ml - 1; j > 0; j--) {
         for (int i = j; i < ml - 1; i++) {
             TRY(restrict_level<double>(h, i + 1));
-            TRY(gs_level<double>(h, i + 1, 0, smoother, 2));
+            TRY(gs_level<double>(h, i + 1, 0, smoother, h->v_down));
         }
-        TRY(gs_level<double>(h, ml - 1, 0, smoother, 20));
+        TRY(gs_level<double>(h, ml - 1, 0, smoother, h->v_bottom));
         for (int i = ml - 1; i >= j; i--) {
             TRY(interp_level<double>(h, i));
-            TRY(gs_level<double>(h, i - 1, 0, smoother, 2));
+            TRY(gs_level<double>(h, i - 1, 0, smoother, h->v_up));
         }
     }
     return PGMG_OK;

@@ -28,6 +28,7 @@ struct CoarsePlan {
     int first, nl;       // levels first..nl-1 run here
     int lu_ok;           // bottom: 1 = explicit-inverse solve, 0 = 24 sweeps
     long long slab_budget;  // slab order of the 8-colour sweeps (as the grid path)
+    int v_down, v_up;       // sweeps on level l: v_down+l before, v_up+l-1 after (multigrid.cc:92,102)
     LevelGeom g[kMaxLv];
     const T* A[kMaxLv];
     T* x[kMaxLv];
@@ -214,15 +215,15 @@ __device__ __forceinline__ void c_lu_apply(const LevelGeom& g, const double* Min
 }
 
 // The V-cycle from level `first` (its source already restricted) to the
-// bottom and back, 8-colour smoothing: 2+l pre- and post-sweeps on level l
-// (multigrid.cc:88-106).  blockDim.x must be a multiple of 32.
+// bottom and back, 8-colour smoothing: v_down+l pre- and v_up+l-1 post-sweeps
+// on level l (multigrid.cc:88-106).  blockDim.x must be a multiple of 32.
 template <class T>
 __global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode) {
     int nth = gridDim.x * blockDim.x;
     int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int nl = P.nl;
     for (int l = P.first; l < nl - 1; l++) {
-        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], 2 + l, mode, P.slab_budget, tid, nth);
+        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.v_down + l, mode, P.slab_budget, tid, nth);
         c_residual<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.res[l], tid, nth);
         cluster_sync();
         c_restrict<T>(P.g[l], P.g[l + 1], P.res[l], P.r[l + 1], P.x[l + 1], tid, nth);
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode)
     for (int l = lb; l > P.first; l--) {
         c_interp<T>(P.g[l - 1], P.g[l], P.x[l - 1], P.x[l], tid, nth);
         cluster_sync();
-        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], 2 + l - 1, mode, P.slab_budget, tid, nth);
+        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], P.v_up + l - 1, mode, P.slab_budget, tid, nth);
     }
 }
 

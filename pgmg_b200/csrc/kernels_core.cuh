@@ -483,6 +483,24 @@ __global__ void __launch_bounds__(kBlock) k_setup_test(LevelGeom g, T* x, T* r, 
     if (xfield) x[g.xi(i, j, k)] = v; else r[g.ri(i, j, k)] = v;
 }
 
+// out = A in (region::mul_A / Ax, region.cc:1861-1912): natural-order input
+// and output of one level, box-order accumulation; neighbours outside the
+// grid carry zero stencil entries and are skipped.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_apply(LevelGeom g, const T* __restrict__ A, const double* __restrict__ in,
+                                                  double* __restrict__ out) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    double acc = 0.0;
+    for (int s = 0; s < 27; s++) {
+        int ii = i + s % 3 - 1, jj = j + (s / 3) % 3 - 1, kk = k + s / 9 - 1;
+        if (ii < 0 || jj < 0 || kk < 0 || ii >= g.m || jj >= g.n || kk >= g.o) continue;
+        acc = __dadd_rn(acc, __dmul_rn((double)A[g.ai(i, j, k, s)], in[g.pi(ii, jj, kk)]));
+    }
+    out[q] = acc;
+}
+
 // Elementwise casts used by mixed precision.
 template <class TI, class TO>
 __global__ void __launch_bounds__(kBlock) k_cast(const TI* __restrict__ in, TO* __restrict__ out, long n) {

@@ -100,3 +100,14 @@ def test_q1_variable_kappa_stencil_symmetric():
     K = kap.reshape(m - 1, m - 1, m - 1)
     h = 1.0 / (m - 1)
     assert C[1, 1, 1, 26] == pytest.approx(-h * K[1, 1, 1] / 12, rel=1e-14)
+
+
+def test_dropin_headers_compile_and_link(tmp_path):
+    """The drop-in C++ headers compile with a driver written against the
+    reference's interface and link against libpgmg_b200.so (no GPU needed)."""
+    import subprocess
+    exe = tmp_path / "dropin_driver"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include", "pgmg"), "-I",
+                    os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "dropin_driver.cc"), "-o",
+                    str(exe), "-L", os.path.join(ROOT, "pgmg_b200"), "-lpgmg_b200"], check=True)
+    assert exe.exists()

@@ -281,3 +281,38 @@ def test_mc8_slab_order_bitwise(mno, budget):
     G.v_cycle(1)
     O.v_cycle(1)
     assert np.array_equal(G.get_x(0), O.get_x(0))
+
+
+def test_apply_matches_oracle_residual():
+    mno = (20, 17, 18)
+    G, prob = make(mno)
+    O = oracle_for(mno, prob, True)
+    v = np.random.default_rng(9).standard_normal(G.npts(0))
+    av = G.apply(0, v)
+    O.set_x(0, v)
+    O.set_r(0, np.zeros(G.npts(0)))
+    # oracle residual with r = 0 is -A v, accumulated in the same order
+    O.set_r(0, np.zeros(G.npts(0)))
+    A = O.get_A27(0)
+    m, n, o = mno
+    ref = np.zeros(m * n * o)
+    x3 = np.pad(v.reshape(o, n, m), 1)
+    for q in range(27):
+        di, dj, dk = q % 3 - 1, (q // 3) % 3 - 1, q // 9 - 1
+        ref += A[:, q] * x3[1 + dk:1 + dk + o, 1 + dj:1 + dj + n, 1 + di:1 + di + m].ravel()
+    assert relerr(av, ref) < 1e-14
+
+
+def test_sweep_count_options():
+    mno = (33, 33, 33)
+    G, prob = make(mno, coarse=P.COARSE_GS, smoother=P.SMOOTH_MC8)
+    assert (G.get_option(P.OPT_V_DOWN), G.get_option(P.OPT_V_UP), G.get_option(P.OPT_V_BOTTOM)) == (2, 2, 20)
+    G.set_option(P.OPT_V_DOWN, 3)
+    G.set_option(P.OPT_V_UP, 1)
+    r0 = G.l2_error_all()
+    G.v_cycle(0)
+    r1 = G.l2_error_all()
+    assert r1 < 1e-2 * r0
+    G2, _ = make(mno, coarse=P.COARSE_GS, smoother=P.SMOOTH_MC8)
+    G2.v_cycle(0)
+    assert not np.array_equal(G.get_x(0), G2.get_x(0))
