@@ -235,6 +235,26 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle *h, double p_scale, int *result,
 pgmg_status pgmg_dev_solve_relres(pgmg_handle *h, double tol, int max_cycles, int check_every,
                                   int *cycles, double *relres);
 
+/* ---- batched solves (many independent problems per launch) ------------- */
+
+/* A batch has slots holding set-up handles (pgmg_dev_build_rat done) of one
+ * precision, 8-colour smoother and default sweep counts; problems of any
+ * size mix.  pgmg_batch_solve solves every attached problem from x = 0 to its
+ * relative residual tol (or max_cycles): each launch of a step covers every
+ * problem still running, per-problem convergence flags live on the device,
+ * and each step is one CUDA graph per batch shape.  A problem's iterates are
+ * bit for bit those of pgmg_dev_solve_relres with check_every = 1.
+ * cycles / relres: per slot, arrays of max_slots (may be NULL).  The results
+ * stay in each handle (pgmg_dev_get_field). */
+typedef struct pgmg_batch pgmg_batch;
+pgmg_status pgmg_batch_create(int max_slots, int precision, int device, pgmg_batch **out);
+pgmg_status pgmg_batch_destroy(pgmg_batch *b);
+const char *pgmg_batch_last_error(pgmg_batch *b);
+pgmg_status pgmg_batch_attach(pgmg_batch *b, int slot, pgmg_handle *h);
+pgmg_status pgmg_batch_detach(pgmg_batch *b, int slot);
+pgmg_status pgmg_batch_solve(pgmg_batch *b, double tol, int max_cycles, int *cycles, double *relres);
+pgmg_status pgmg_batch_launch_count(pgmg_batch *b, long long *n);
+
 /* ---- host problem generators (no GPU needed) ---------------------------- */
 
 /* Cell-centred kappa = exp(sigma*g), g a seeded Gaussian field smoothed by a

@@ -90,6 +90,13 @@ SIGNATURES = [
     ("pgmg_dev_norms", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pgmg_dev_solve_v_cycles", C.c_int, [_VP, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("pgmg_dev_solve_relres", C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("pgmg_batch_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("pgmg_batch_destroy", C.c_int, [_VP]),
+    ("pgmg_batch_last_error", C.c_char_p, [_VP]),
+    ("pgmg_batch_attach", C.c_int, [_VP, C.c_int, _VP]),
+    ("pgmg_batch_detach", C.c_int, [_VP, C.c_int]),
+    ("pgmg_batch_solve", C.c_int, [_VP, C.c_double, C.c_int, _VP, _VP]),
+    ("pgmg_batch_launch_count", C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     ("pgmg_problem_kappa", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_double, _dp]),
     ("pgmg_problem_q1", C.c_int, [C.c_int, C.c_int, C.c_int, _VP, _dp, _VP]),
     ("pgmg_problem_rhs", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, _dp]),
@@ -375,3 +382,54 @@ class Multigrid:
         self._ck(lib().pgmg_dev_solve_relres(self._h, tol, max_cycles, check_every, C.byref(cyc), C.byref(rr)),
                  "solve")
         return cyc.value, rr.value
+
+
+class Batch:
+    """Slots of set-up ``Multigrid`` objects solved together (one launch per
+    level/colour across all problems; see pgmg_batch_* in pgmg_dev.h)."""
+
+    def __init__(self, max_slots: int, precision: int = MIXED, device: int = -1):
+        self.max_slots = max_slots
+        self._b = None
+        b = C.c_void_p()
+        st = lib().pgmg_batch_create(max_slots, precision, device, C.byref(b))
+        if st:
+            raise PgmgError(st, "pgmg_batch_create")
+        self._b = b
+        self._members = {}
+
+    def _ck(self, st, where):
+        if st:
+            detail = lib().pgmg_batch_last_error(self._b)
+            raise PgmgError(st, where, detail.decode() if detail else "")
+
+    def attach(self, slot: int, mg: "Multigrid"):
+        self._ck(lib().pgmg_batch_attach(self._b, slot, mg.handle), "batch_attach")
+        self._members[slot] = mg
+
+    def detach(self, slot: int):
+        self._ck(lib().pgmg_batch_detach(self._b, slot), "batch_detach")
+        self._members.pop(slot, None)
+
+    def solve(self, tol: float = 1e-10, max_cycles: int = 100):
+        cyc = np.zeros(self.max_slots, np.int32)
+        rr = np.zeros(self.max_slots)
+        self._ck(lib().pgmg_batch_solve(self._b, tol, max_cycles, _ptr(cyc), _ptr(rr)), "batch_solve")
+        return cyc, rr
+
+    @property
+    def launches(self) -> int:
+        v = C.c_longlong()
+        self._ck(lib().pgmg_batch_launch_count(self._b, C.byref(v)), "batch_launch_count")
+        return v.value
+
+    def close(self):
+        if self._b is not None:
+            lib().pgmg_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -15,81 +15,7 @@
 
 using namespace pgmg;
 
-namespace {
-
-constexpr int kMaxLevels = 16;      // mg_max_levels, common.hh:15
-constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
-constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
-constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
-constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
-constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
-constexpr int kClusterThreads = 512;
-
-struct Level {
-    LevelGeom g;
-    double *A64 = nullptr, *x64 = nullptr, *r64 = nullptr, *res64 = nullptr;
-    float *A32 = nullptr, *x32 = nullptr, *r32 = nullptr, *res32 = nullptr;
-    int8_t* S = nullptr;
-};
-
-template <class T> struct View { T *A, *x, *r, *res; };
-inline View<double> view64(Level& L) { return {L.A64, L.x64, L.r64, L.res64}; }
-inline View<float> view32(Level& L) { return {L.A32, L.x32, L.r32, L.res32}; }
-
-inline long nblk(long n, int b = kBlock) { return (n + b - 1) / b; }
-
-// Simple bump allocator over one device allocation (256-byte aligned).
-struct Arena {
-    char* base = nullptr;
-    size_t size = 0, used = 0;
-    template <class T> T* take(size_t count) {
-        size_t bytes = (count * sizeof(T) + 255) / 256 * 256;
-        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
-        used += bytes;
-        return p;
-    }
-};
-
-}  // namespace
-
-struct pgmg_handle {
-    pgmg_dims dims{};
-    int device = 0;
-    cudaStream_t own = nullptr, stream = nullptr;
-    int nl = 0;
-    Level L[kMaxLevels];
-    Arena arena;
-    // coarsest level
-    long nex = 0;
-    double *M = nullptr, *Minv = nullptr, *lubuf = nullptr;
-    int *piv = nullptr, *info = nullptr;
-    int lu_ok = 0;
-    bool uploaded = false, built = false;
-    // staging and reductions
-    double* stage = nullptr;
-    size_t stage_elems = 0;
-    double* partials = nullptr;
-    double* norm_dev = nullptr;
-    double* norm_host = nullptr;  // pinned, 2 doubles
-    // mg_guide state (multigrid.hh:34-118)
-    int period = 16, iter = 16, use_avg = 0, tol_set = 0;
-    double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;
-    long long launches = 0;  // kernels this handle has launched
-    bool x0_zero = true;     // level-0 x known to be zero (cleared, not written since)
-    double last_rho = 0;     // per-cycle residual reduction seen by the last solve
-    // Captured V-cycles, by [float][mode][smoother].
-    cudaGraphExec_t vgraph[2][2][2] = {};
-    long long vgraph_nodes[2][2][2] = {};
-    bool use_graphs = true;
-    // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
-    // first level it handles.
-    int cluster_size = 0;
-    int coarse_first = 0;
-    long long slab_budget = 0;  // bytes of x per slab of the 8-colour sweep (0 = one slab)
-    // Public sweep counts of the reference's multigrid (multigrid.hh:122-128).
-    int v_down = 2, v_up = 2, v_bottom = 20;
-    char err[512] = {0};
-};
+#include "handle.cuh"
 
 namespace {
 
@@ -164,6 +90,8 @@ void carve(pgmg_handle* h) {
         h->piv = a.take<int>(n);
     }
     h->info = a.take<int>(4);
+    h->plan64 = a.take<CoarsePlan<double>>(1);
+    h->plan32 = a.take<CoarsePlan<float>>(1);
     h->partials = a.take<double>(2 * maxblocks);
     h->norm_dev = a.take<double>(2);
     const LevelGeom& g0 = h->L[0].g;
@@ -286,9 +214,9 @@ pgmg_status coarse_solve_t(pgmg_handle* h, int smoother) {
     return gs_level<T>(h, lb, 0, smoother, kGsExact);
 }
 
+// Fills the coarse-cycle plan of a handle (host copy).
 template <class T>
-pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
-    CoarsePlan<T> P;
+void fill_plan(pgmg_handle* h, int first, CoarsePlan<T>& P) {
     P.first = first;
     P.nl = h->nl;
     P.lu_ok = h->lu_ok;
@@ -301,6 +229,29 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
         P.g[l] = h->L[l].g;
         P.A[l] = v.A; P.x[l] = v.x; P.r[l] = v.r; P.res[l] = v.res;
     }
+}
+
+// Refreshes the device copies of the plans (after set-up and option changes).
+pgmg_status upload_plans(pgmg_handle* h) {
+    CoarsePlan<double> p64;
+    fill_plan<double>(h, h->coarse_first, p64);
+    CK(cudaMemcpyAsync(h->plan64, &p64, sizeof(p64), cudaMemcpyHostToDevice, h->stream));
+    if (h->dims.precision == PGMG_MIXED) {
+        CoarsePlan<float> p32;
+        fill_plan<float>(h, h->coarse_first, p32);
+        CK(cudaMemcpyAsync(h->plan32, &p32, sizeof(p32), cudaMemcpyHostToDevice, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return PGMG_OK;
+}
+
+template <class T> const CoarsePlan<T>* plan_of(pgmg_handle* h);
+template <> const CoarsePlan<double>* plan_of<double>(pgmg_handle* h) { return h->plan64; }
+template <> const CoarsePlan<float>* plan_of<float>(pgmg_handle* h) { return h->plan32; }
+
+template <class T>
+pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
+    (void)first;  // the device plan carries h->coarse_first
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(h->cluster_size, 1, 1);
     cfg.blockDim = dim3(kClusterThreads, 1, 1);
@@ -312,7 +263,9 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, P, mode));
+    const int* no_map = nullptr;
+    const int* no_flags = nullptr;
+    CK(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, plan_of<T>(h), no_map, no_flags, mode));
     h->launches++;
     return PGMG_OK;
 }
@@ -616,34 +569,33 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
     if (!h) return PGMG_ERR_ARG;
     switch (key) {
         case PGMG_OPT_GRAPHS:
-            drop_graphs(h);
             h->use_graphs = value != 0;
-            return PGMG_OK;
+            break;
         case PGMG_OPT_CLUSTER_FIRST:
             if (value < 0 || value > h->nl) return fail(h, PGMG_ERR_ARG, "cluster level %lld out of range", value);
-            drop_graphs(h);
             h->coarse_first = (int)value;
-            return PGMG_OK;
-        case PGMG_OPT_SLAB_BUDGET:
-            drop_graphs(h);
-            h->slab_budget = value;
-            return PGMG_OK;
-        case PGMG_OPT_V_DOWN:
-        case PGMG_OPT_V_UP:
-        case PGMG_OPT_V_BOTTOM:
-            if (value < 0 || value > 1000) return fail(h, PGMG_ERR_ARG, "sweep count %lld out of range", value);
-            drop_graphs(h);
-            (key == PGMG_OPT_V_DOWN ? h->v_down : key == PGMG_OPT_V_UP ? h->v_up : h->v_bottom) = (int)value;
-            return PGMG_OK;
+            break;
         case PGMG_OPT_CLUSTER_SIZE:
             if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
             if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
                 return fail(h, PGMG_ERR_UNSUPPORTED, "cluster of %lld CTAs not launchable", value);
-            drop_graphs(h);
             h->cluster_size = (int)value;
-            return PGMG_OK;
+            break;
+        case PGMG_OPT_SLAB_BUDGET:
+            h->slab_budget = value;
+            break;
+        case PGMG_OPT_V_DOWN:
+        case PGMG_OPT_V_UP:
+        case PGMG_OPT_V_BOTTOM:
+            if (value < 0 || value > 1000) return fail(h, PGMG_ERR_ARG, "sweep count %lld out of range", value);
+            (key == PGMG_OPT_V_DOWN ? h->v_down : key == PGMG_OPT_V_UP ? h->v_up : h->v_bottom) = (int)value;
+            break;
+        default:
+            return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
     }
-    return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
+    drop_graphs(h);
+    if (h->built) TRY(upload_plans(h));
+    return PGMG_OK;
 }
 
 pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
@@ -761,6 +713,7 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
         }
     TRY(lu_setup(h));
     CK(cudaStreamSynchronize(h->stream));
+    TRY(upload_plans(h));
     h->built = true;
     return PGMG_OK;
 }

@@ -1,0 +1,89 @@
+// Internal: the handle behind pgmg_handle* and its per-level buffers, shared
+// by the single-problem entry points (capi.cu) and the batched solver
+// (batch.cu).
+#pragma once
+#include "../../include/pgmg_dev.h"
+#include "kernels_coarse.cuh"
+#include "kernels_core.cuh"
+#include "layout.cuh"
+
+namespace pgmg {
+constexpr int kMaxLevels = 16;      // mg_max_levels, common.hh:15
+constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
+constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
+constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
+constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
+constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
+constexpr int kClusterThreads = 512;
+
+struct Level {
+    LevelGeom g;
+    double *A64 = nullptr, *x64 = nullptr, *r64 = nullptr, *res64 = nullptr;
+    float *A32 = nullptr, *x32 = nullptr, *r32 = nullptr, *res32 = nullptr;
+    int8_t* S = nullptr;
+};
+
+template <class T> struct View { T *A, *x, *r, *res; };
+inline View<double> view64(Level& L) { return {L.A64, L.x64, L.r64, L.res64}; }
+inline View<float> view32(Level& L) { return {L.A32, L.x32, L.r32, L.res32}; }
+
+__host__ __device__ inline long nblk(long n, int b = kBlock) { return (n + b - 1) / b; }
+
+// Simple bump allocator over one device allocation (256-byte aligned).
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T> T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) / 256 * 256;
+        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += bytes;
+        return p;
+    }
+};
+
+}  // namespace pgmg
+
+struct pgmg_handle {
+    using Level = pgmg::Level;
+    using Arena = pgmg::Arena;
+    pgmg_dims dims{};
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    int nl = 0;
+    Level L[pgmg::kMaxLevels];
+    Arena arena;
+    // coarsest level
+    long nex = 0;
+    double *M = nullptr, *Minv = nullptr, *lubuf = nullptr;
+    int *piv = nullptr, *info = nullptr;
+    int lu_ok = 0;
+    bool uploaded = false, built = false;
+    // staging and reductions
+    double* stage = nullptr;
+    size_t stage_elems = 0;
+    double* partials = nullptr;
+    double* norm_dev = nullptr;
+    double* norm_host = nullptr;  // pinned, 2 doubles
+    // mg_guide state (multigrid.hh:34-118)
+    int period = 16, iter = 16, use_avg = 0, tol_set = 0;
+    double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;
+    long long launches = 0;  // kernels this handle has launched
+    bool x0_zero = true;     // level-0 x known to be zero (cleared, not written since)
+    double last_rho = 0;     // per-cycle residual reduction seen by the last solve
+    // Captured V-cycles, by [float][mode][smoother].
+    cudaGraphExec_t vgraph[2][2][2] = {};
+    long long vgraph_nodes[2][2][2] = {};
+    bool use_graphs = true;
+    // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
+    // first level it handles.
+    int cluster_size = 0;
+    int coarse_first = 0;
+    long long slab_budget = 0;  // bytes of x per slab of the 8-colour sweep (0 = one slab)
+    // Device copies of the coarse-cycle plans (CoarsePlan<double>, <float>).
+    pgmg::CoarsePlan<double>* plan64 = nullptr;
+    pgmg::CoarsePlan<float>* plan32 = nullptr;
+    // Public sweep counts of the reference's multigrid (multigrid.hh:122-128).
+    int v_down = 2, v_up = 2, v_bottom = 20;
+    char err[512] = {0};
+};
+

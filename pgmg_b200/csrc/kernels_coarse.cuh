@@ -216,11 +216,23 @@ __device__ __forceinline__ void c_lu_apply(const LevelGeom& g, const double* Min
 
 // The V-cycle from level `first` (its source already restricted) to the
 // bottom and back, 8-colour smoothing: v_down+l pre- and v_up+l-1 post-sweeps
-// on level l (multigrid.cc:88-106).  blockDim.x must be a multiple of 32.
+// on level l (multigrid.cc:88-106).  One cluster per problem: cluster c runs
+// plans[slot_of_cluster[c]] (plans[c] if the map is null) and returns at once
+// if that problem's active flag is 0.  blockDim.x must be a multiple of 32.
 template <class T>
-__global__ void __launch_bounds__(512) k_coarse_cycle(CoarsePlan<T> P, int mode) {
-    int nth = gridDim.x * blockDim.x;
-    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(512) k_coarse_cycle(const CoarsePlan<T>* __restrict__ plans,
+                                                      const int* __restrict__ slot_of_cluster,
+                                                      const int* __restrict__ active, int mode) {
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    int csize = (int)cl.num_blocks();
+    int cid = blockIdx.x / csize;
+    int slot = slot_of_cluster ? slot_of_cluster[cid] : cid;
+    // The flag is uniform across the cluster (written by an earlier kernel),
+    // so either every CTA of the cluster returns here or none does.
+    if (active && !active[slot]) return;
+    const CoarsePlan<T>& P = plans[slot];
+    int nth = csize * blockDim.x;
+    int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
     int nl = P.nl;
     for (int l = P.first; l < nl - 1; l++) {
         c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.v_down + l, mode, P.slab_budget, tid, nth);

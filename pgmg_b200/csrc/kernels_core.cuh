@@ -34,11 +34,11 @@ __device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ 
 // the 26 neighbours read here belong to other colours and are not written
 // by this launch.  One thread per colour point; coefficient slot q of
 // consecutive threads is contiguous (structure-of-arrays per colour).
-template <class T, bool EXACT>
-__global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
-                                                      const T* __restrict__ A, int col, int k2lo, int k2hi) {
-    long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (p >= (long)k2hi * g.M2 * g.N2) return;
+// One colour point p (index inside colour `col`): the body of k_gs_colour,
+// shared with the batched kernels.
+template <class T>
+__device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* __restrict__ r,
+                                             const T* __restrict__ A, int col, long p) {
     int i2 = (int)(p % g.M2);
     long t = p / g.M2;
     int j2 = (int)(t % g.N2);
@@ -48,8 +48,16 @@ __global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T
     uint64_t ps = policy_evict_first(), pk = policy_evict_last();
     long xc = g.xi(i, j, k);
     const T* Ap = A + (long)col * 27 * g.Nc + p;
-    T v = gs_value<T, EXACT>(g, x, xc, Ap, g.Nc, ld_stream(r + (long)col * g.Nc + p, ps), ps, pk);
+    T v = gs_value<T, true>(g, x, xc, Ap, g.Nc, ld_stream(r + (long)col * g.Nc + p, ps), ps, pk);
     st_keep(x + xc, v, pk);
+}
+
+template <class T, bool EXACT>
+__global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
+                                                      const T* __restrict__ A, int col, int k2lo, int k2hi) {
+    long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (p >= (long)k2hi * g.M2 * g.N2) return;
+    gs_colour_at<T>(g, x, r, A, col, p);
 }
 
 // Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of
@@ -208,36 +216,45 @@ __device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
 // box order, region.cc:1833-1842), written colour-major to `out` (type TO),
 // with per-block partial sums of res^2 and r^2 (region.cc:1475-1490,
 // 1549-1558) when `partials` is non-null.  Grid: (blocks per colour, 8).
+// Residual of colour point p of colour col: writes r - Ax to out (if
+// non-null) and adds res^2 and r^2 to the accumulators.
+template <class T, class TO>
+__device__ __forceinline__ void residual_at(const LevelGeom& g, const T* __restrict__ x, const T* __restrict__ r,
+                                            const T* __restrict__ A, TO* __restrict__ out, int col, long p,
+                                            double& s_res, double& s_rhs) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    if (p >= nc) return;
+    int i2 = (int)(p % g.M2);
+    long t = p / g.M2;
+    int j2 = (int)(t % g.N2);
+    int k2 = (int)(t / g.N2);
+    int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+    if (i >= g.m || j >= g.n || k >= g.o) return;
+    uint64_t ps = policy_evict_first(), pk = policy_evict_last();
+    long xc = g.xi(i, j, k);
+    const T* Ap = A + (long)col * 27 * g.Nc + p;
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 27; q++)
+        acc = madd<true, T>(acc, ld_stream(Ap + q * g.Nc, ps), ld_keep(x + xc + slot_off(g, q), pk));
+    T rv = ld_stream(r + (long)col * g.Nc + p, ps);
+    T res = sub_rn<T>(rv, acc);
+    if (out) out[(long)col * g.Nc + p] = (TO)res;
+    s_res = (double)res * (double)res;
+    s_rhs = (double)rv * (double)rv;
+}
+
+// K5 / residual half of K3: res = r - A x over a whole level (all 27 slots in
+// box order, region.cc:1833-1842), written colour-major to `out` (type TO),
+// with per-block partial sums of res^2 and r^2 (region.cc:1475-1490,
+// 1549-1558) when `partials` is non-null.  Grid: (blocks per colour, 8).
 template <class T, class TO, bool EXACT>
 __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __restrict__ x,
                                                      const T* __restrict__ r, const T* __restrict__ A,
                                                      TO* __restrict__ out, double* __restrict__ partials) {
     __shared__ double sh[64];
-    int col = blockIdx.y;
-    long nc = (long)g.M2 * g.N2 * g.O2;
-    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
     double s_res = 0, s_rhs = 0;
-    if (p < nc) {
-        int i2 = (int)(p % g.M2);
-        long t = p / g.M2;
-        int j2 = (int)(t % g.N2);
-        int k2 = (int)(t / g.N2);
-        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
-        if (i < g.m && j < g.n && k < g.o) {
-            uint64_t ps = policy_evict_first(), pk = policy_evict_last();
-            long xc = g.xi(i, j, k);
-            const T* Ap = A + (long)col * 27 * g.Nc + p;
-            T acc = T(0);
-#pragma unroll
-            for (int q = 0; q < 27; q++)
-                acc = madd<EXACT, T>(acc, ld_stream(Ap + q * g.Nc, ps), ld_keep(x + xc + slot_off(g, q), pk));
-            T rv = ld_stream(r + (long)col * g.Nc + p, ps);
-            T res = EXACT ? sub_rn<T>(rv, acc) : rv - acc;
-            if (out) out[(long)col * g.Nc + p] = (TO)res;
-            s_res = (double)res * (double)res;
-            s_rhs = (double)rv * (double)rv;
-        }
-    }
+    residual_at<T, TO>(g, x, r, A, out, blockIdx.y, blockIdx.x * (long)blockDim.x + threadIdx.x, s_res, s_rhs);
     if (partials) {
         block_sum2(s_res, s_rhs, sh);
         if (threadIdx.x == 0) {
@@ -274,7 +291,7 @@ __global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restr
 }
 
 // Sums nb partial pairs in a fixed order into out[0], out[1].
-__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partials, long nb,
+static __global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partials, long nb,
                                                           double* __restrict__ out) {
     __shared__ double sh[64];
     double a = 0, b = 0;
@@ -292,9 +309,8 @@ __global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restri
 // (ti,tj+1,tk+1) point (region.cc:888-895); that is kept, see ysnap below.
 // Also clears the coarse x (multigrid.cc:219).
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
-                                                     T* __restrict__ rc, T* __restrict__ xc) {
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
+                                            T* __restrict__ rc, T* __restrict__ xc, long q) {
     if (q >= gc.npts) return;
     int I = (int)(q % gc.m);
     long t = q / gc.m;
@@ -334,15 +350,20 @@ __global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc,
     xc[gc.xi(I, J, K)] = T(0);
 }
 
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
+                                                     T* __restrict__ rc, T* __restrict__ xc) {
+    restrict_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
 // Interpolation with correction add (region.cc:576-593): each fine point
 // belongs to exactly one 2x2x2 cube (C = t>>1, role t&1 per axis) and gets
 // the value interpolate_full (:752-772) or interpolate_partial (:779-810)
 // would give it -- the two differ in how some sums associate; partial is
 // used on the last cube of every row, row of every slice and slice.
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
-                                                   const T* __restrict__ xcv) {
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& gc, T* __restrict__ xf,
+                                          const T* __restrict__ xcv, long q) {
     if (q >= gf.npts) return;
     int i = (int)(q % gf.m);
     long t = q / gf.m;
@@ -389,6 +410,12 @@ __global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T
     }
     long xf_i = gf.xi(i, j, k);
     xf[xf_i] = xf[xf_i] + val;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
+                                                   const T* __restrict__ xcv) {
+    interp_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,7 +536,7 @@ __global__ void __launch_bounds__(kBlock) k_cast(const TI* __restrict__ in, TO* 
 }
 
 // x64 += x32 over the interior (FP64 update of iterative refinement).
-__global__ void __launch_bounds__(kBlock) k_add_correction(LevelGeom g, double* __restrict__ x64,
+static __global__ void __launch_bounds__(kBlock) k_add_correction(LevelGeom g, double* __restrict__ x64,
                                                            const float* __restrict__ e32) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
