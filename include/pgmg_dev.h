@@ -109,6 +109,11 @@ typedef struct {
  * arena.  Replaces multigrid(p_class&,geometry&,comm_buffer&)
  * (multigrid.hh:283-295) minus the problem-class callbacks. */
 pgmg_status pgmg_dev_create(const pgmg_dims *dims, pgmg_handle **out);
+/* As pgmg_dev_create, but the handle lives inside caller-owned device memory
+ * `mem` (256-byte aligned, at least pgmg_dev_plan_bytes bytes) and never
+ * allocates or frees device memory itself -- for servers that manage one
+ * pool and must not stall the device in cudaMalloc/cudaFree. */
+pgmg_status pgmg_dev_create_in(const pgmg_dims *dims, void *mem, size_t bytes, pgmg_handle **out);
 /* Frees everything (multigrid::~multigrid, multigrid.cc:7-14). */
 pgmg_status pgmg_dev_destroy(pgmg_handle *h);
 /* Issue all further work of the handle on this cudaStream_t (NULL = the
@@ -164,6 +169,15 @@ pgmg_status pgmg_dev_plan_bytes(const pgmg_dims *dims, size_t *bytes);
  * (region.hh:96-101) and the top-level constructor's box pass
  * (region.hh:492-519). */
 pgmg_status pgmg_dev_upload_level0(pgmg_handle *h, const double *coef27, const int *S6);
+/* Level-0 Q1 FEM stencils of -div(kappa grad u) assembled on the device from
+ * a cell field ((m-1)(n-1)(o-1) doubles, natural order, host or device):
+ * kappa itself (from_log = 0; NULL = constant 1) or g with kappa =
+ * exp(sigma*g) (from_log = 1).  Same stencils, boxes and Dirichlet fix rows
+ * as pgmg_problem_q1 followed by pgmg_dev_upload_level0, with 27x less data
+ * to move. */
+pgmg_status pgmg_dev_assemble_q1(pgmg_handle *h, const double *cells, int from_log, double sigma);
+/* Level-0 source = pgmg_problem_rhs(m, n, o, seed), generated on the device. */
+pgmg_status pgmg_dev_rhs_uniform(pgmg_handle *h, uint64_t seed);
 /* Galerkin coarse operators A_c = (1/8) P^T A_f P on the device for every
  * level, the coarse boxes, and the coarsest-level LU.  Replaces
  * multigrid::compute_rats (multigrid.cc:138-152), region::fill_rat_bounds
@@ -264,6 +278,9 @@ int pgmg_problem_kappa(int m, int n, int o, double sigma, uint64_t seed, double 
 /* Q1 trilinear FEM stencils of -div(kappa grad u) (kappa NULL = 1) with
  * Dirichlet fix rows on the boundary; fills coef27 and, if non-NULL, S6. */
 int pgmg_problem_q1(int m, int n, int o, const double *kappa, double *coef27, int *S6);
+/* The normalised smoothed Gaussian field g of pgmg_problem_kappa (kappa =
+ * exp(sigma*g)), cells natural order. */
+int pgmg_problem_gauss(int m, int n, int o, uint64_t seed, double width, double *g);
 /* Right-hand side: interior nodes uniform[-1,1] from the seed, boundary 0. */
 int pgmg_problem_rhs(int m, int n, int o, uint64_t seed, double *r);
 

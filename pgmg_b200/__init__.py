@@ -97,6 +97,10 @@ SIGNATURES = [
     ("pgmg_batch_detach", C.c_int, [_VP, C.c_int]),
     ("pgmg_batch_solve", C.c_int, [_VP, C.c_double, C.c_int, _VP, _VP]),
     ("pgmg_batch_launch_count", C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    ("pgmg_dev_create_in", C.c_int, [C.POINTER(Dims), _VP, C.c_size_t, C.POINTER(C.c_void_p)]),
+    ("pgmg_dev_assemble_q1", C.c_int, [_VP, _VP, C.c_int, C.c_double]),
+    ("pgmg_dev_rhs_uniform", C.c_int, [_VP, C.c_uint64]),
+    ("pgmg_problem_gauss", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_double, _dp]),
     ("pgmg_problem_kappa", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_double, _dp]),
     ("pgmg_problem_q1", C.c_int, [C.c_int, C.c_int, C.c_int, _VP, _dp, _VP]),
     ("pgmg_problem_rhs", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, _dp]),
@@ -130,6 +134,15 @@ def problem_kappa(m: int, n: int, o: int, sigma: float, seed: int, width: float 
     st = lib().pgmg_problem_kappa(m, n, o, float(sigma), int(seed), float(width), out)
     if st:
         raise PgmgError(st, "pgmg_problem_kappa")
+    return out
+
+
+def problem_gauss(m: int, n: int, o: int, seed: int, width: float = 8.0) -> np.ndarray:
+    """The normalised smoothed Gaussian cell field g (kappa = exp(sigma*g))."""
+    out = np.empty((m - 1) * (n - 1) * (o - 1))
+    st = lib().pgmg_problem_gauss(m, n, o, int(seed), float(width), out)
+    if st:
+        raise PgmgError(st, "pgmg_problem_gauss")
     return out
 
 
@@ -170,13 +183,18 @@ class Multigrid:
     """One multigrid hierarchy on one GPU (see module docstring)."""
 
     def __init__(self, m: int, n: int, o: int, precision: int = FP64, coarse: int = COARSE_LU,
-                 smoother: int = SMOOTH_MC8, device: int = -1, prd=(False, False, False)):
+                 smoother: int = SMOOTH_MC8, device: int = -1, prd=(False, False, False), mem=None):
+        """mem: optional (device pointer, bytes) the handle lives in (no
+        device allocation of its own; see pgmg_dev_create_in)."""
         self.m, self.n, self.o = m, n, o
         self.precision, self.coarse, self.smoother = precision, coarse, smoother
         self._h = None
         d = Dims(m, n, o, int(prd[0]), int(prd[1]), int(prd[2]), precision, coarse, smoother, device)
         h = C.c_void_p()
-        st = lib().pgmg_dev_create(C.byref(d), C.byref(h))
+        if mem is None:
+            st = lib().pgmg_dev_create(C.byref(d), C.byref(h))
+        else:
+            st = lib().pgmg_dev_create_in(C.byref(d), mem[0], mem[1], C.byref(h))
         if st:
             raise PgmgError(st, "pgmg_dev_create")
         self._h = h
@@ -264,6 +282,24 @@ class Multigrid:
             sp = _ptr(S6)
         self._ck(lib().pgmg_dev_upload_level0(self._h, cp, sp), "upload_level0")
         self._ck(lib().pgmg_dev_build_rat(self._h), "build_rat")
+
+    def assemble_q1(self, cells=None, from_log: bool = False, sigma: float = 1.0, build: bool = True):
+        """Level-0 Q1 stencils assembled on the GPU from a cell field (kappa,
+        or g with kappa = exp(sigma*g)); host array or device pointer."""
+        if cells is None:
+            cp = None
+        elif isinstance(cells, int):
+            cp = cells
+        else:
+            cells = np.ascontiguousarray(cells, np.float64)
+            cp = _ptr(cells)
+        self._ck(lib().pgmg_dev_assemble_q1(self._h, cp, int(from_log), float(sigma)), "assemble_q1")
+        if build:
+            self._ck(lib().pgmg_dev_build_rat(self._h), "build_rat")
+
+    def rhs_uniform(self, seed: int):
+        """Level-0 source = problem_rhs(m, n, o, seed), generated on the GPU."""
+        self._ck(lib().pgmg_dev_rhs_uniform(self._h, int(seed)), "rhs_uniform")
 
     @property
     def lu_enabled(self) -> bool:

@@ -9,13 +9,9 @@
 #include <vector>
 
 #include "../../include/pgmg_dev.h"
-#include "kernels_coarse.cuh"
-#include "kernels_core.cuh"
-#include "kernels_setup.cuh"
+#include "handle.cuh"
 
 using namespace pgmg;
-
-#include "handle.cuh"
 
 namespace {
 
@@ -90,6 +86,7 @@ void carve(pgmg_handle* h) {
         h->piv = a.take<int>(n);
     }
     h->info = a.take<int>(4);
+    h->lu_scratch = a.take<double>(64);
     h->plan64 = a.take<CoarsePlan<double>>(1);
     h->plan32 = a.take<CoarsePlan<float>>(1);
     h->partials = a.take<double>(2 * maxblocks);
@@ -295,6 +292,29 @@ int probe_cluster(int size) {
     return n;
 }
 
+int probe_lu_cluster(int size) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(size, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (size > 8 && cudaFuncSetAttribute(k_lu_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, k_lu_cluster, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nc;
+}
+
 // One V-cycle (multigrid::v_cycle, multigrid.cc:88-106).  With the 8-colour
 // smoother the levels from h->coarse_first down run as one cluster kernel;
 // the LU-exact coarse solve and the lexicographic smoother use the grid
@@ -411,13 +431,30 @@ pgmg_status lu_setup(pgmg_handle* h) {
     CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 4, h->stream));
     k_lu_build<<<nblk(n * 27), kBlock, 0, h->stream>>>(L.g, L.A64, h->M);
     CKL();
-    for (int j = 0; j < n; j++) {
-        k_lu_pivot<<<1, 1024, 0, h->stream>>>(h->M, (int)n, j, h->piv, h->info);
-        CKL();
-        long rem = n - j - 1;
-        if (rem > 0) {
-            k_lu_update<<<nblk(rem * rem), kBlock, 0, h->stream>>>(h->M, (int)n, j);
+    if (h->cluster_size > 0) {
+        // One cluster kernel for the whole factorisation.
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(h->cluster_size, 1, 1);
+        cfg.blockDim = dim3(512, 1, 1);
+        cfg.stream = h->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = h->cluster_size;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_lu_cluster, h->M, (int)n, h->piv, h->info, h->lu_scratch));
+        h->launches++;
+    } else {
+        for (int j = 0; j < n; j++) {
+            k_lu_pivot<<<1, 1024, 0, h->stream>>>(h->M, (int)n, j, h->piv, h->info);
             CKL();
+            long rem = n - j - 1;
+            if (rem > 0) {
+                k_lu_update<<<nblk(rem * rem), kBlock, 0, h->stream>>>(h->M, (int)n, j);
+                CKL();
+            }
         }
     }
     int info = 0;
@@ -477,7 +514,7 @@ pgmg_status pgmg_dev_plan_bytes(const pgmg_dims* dims, size_t* bytes) {
     return PGMG_OK;
 }
 
-pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
+static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_bytes, pgmg_handle** out) {
     if (!dims || !out) return PGMG_ERR_ARG;
     *out = nullptr;
     if (dims->m < 2 || dims->n < 2 || dims->o < 2) return PGMG_ERR_ARG;
@@ -501,23 +538,31 @@ pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
     for (int l = 0; l < h->nl; l++) h->L[l].g = g[l];
     carve(h);  // count
     size_t bytes = h->arena.used;
-    cudaError_t e = cudaMalloc(&h->arena.base, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        delete h;
-        return PGMG_ERR_MEMORY;
+    if (mem) {
+        if (mem_bytes < bytes || (reinterpret_cast<uintptr_t>(mem) & 255)) {
+            delete h;
+            return PGMG_ERR_MEMORY;
+        }
+        h->arena.base = static_cast<char*>(mem);
+        h->own_arena = false;
+    } else {
+        cudaError_t e = cudaMalloc(&h->arena.base, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            delete h;
+            return PGMG_ERR_MEMORY;
+        }
     }
     h->arena.size = bytes;
     carve(h);  // assign
-    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost(&h->norm_host, 2 * sizeof(double)) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         pgmg_dev_destroy(h);
         return PGMG_ERR_CUDA;
     }
     h->stream = h->own;
     for (int size : {16, 8}) {
-        if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0) {
+        if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0 && probe_lu_cluster(size) > 0) {
             h->cluster_size = size;
             break;
         }
@@ -534,12 +579,18 @@ pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) {
     return PGMG_OK;
 }
 
+pgmg_status pgmg_dev_create(const pgmg_dims* dims, pgmg_handle** out) { return create_common(dims, nullptr, 0, out); }
+
+pgmg_status pgmg_dev_create_in(const pgmg_dims* dims, void* mem, size_t bytes, pgmg_handle** out) {
+    if (!mem) return PGMG_ERR_ARG;
+    return create_common(dims, mem, bytes, out);
+}
+
 pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    if (h->arena.base) cudaFree(h->arena.base);
-    if (h->norm_host) cudaFreeHost(h->norm_host);
+    if (h->arena.base && h->own_arena) cudaFree(h->arena.base);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
     return PGMG_OK;
@@ -690,6 +741,37 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
     CK(cudaStreamSynchronize(h->stream));  // s8 and the caller's array are released on return
     h->uploaded = true;
     h->built = false;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_assemble_q1(pgmg_handle* h, const double* cells, int from_log, double sigma) {
+    if (!h) return PGMG_ERR_ARG;
+    Level& L = h->L[0];
+    const LevelGeom& g = L.g;
+    const double* dc = nullptr;
+    if (cells) {
+        size_t nc = (size_t)(g.m - 1) * (g.n - 1) * (g.o - 1);
+        if (is_device_ptr(cells)) dc = cells;
+        else {
+            CK(cudaMemcpyAsync(h->stage, cells, nc * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            dc = h->stage;
+        }
+    }
+    int mx = g.m > g.n ? (g.m > g.o ? g.m : g.o) : (g.n > g.o ? g.n : g.o);
+    double hh = 1.0 / (double)(mx - 1);
+    k_assemble_q1<<<nblk(g.npts, 128), 128, 0, h->stream>>>(g, dc, from_log, sigma, hh, L.A64, L.S);
+    CKL();
+    CK(cudaStreamSynchronize(h->stream));
+    h->uploaded = true;
+    h->built = false;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_dev_rhs_uniform(pgmg_handle* h, uint64_t seed) {
+    if (!h) return PGMG_ERR_ARG;
+    Level& L = h->L[0];
+    k_rhs_uniform<<<nblk(L.g.npts), 256, 0, h->stream>>>(L.g, seed, L.r64);
+    CKL();
     return PGMG_OK;
 }
 

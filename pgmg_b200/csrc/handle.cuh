@@ -5,6 +5,7 @@
 #include "../../include/pgmg_dev.h"
 #include "kernels_coarse.cuh"
 #include "kernels_core.cuh"
+#include "kernels_setup.cuh"
 #include "layout.cuh"
 
 namespace pgmg {
@@ -63,7 +64,9 @@ struct pgmg_handle {
     size_t stage_elems = 0;
     double* partials = nullptr;
     double* norm_dev = nullptr;
-    double* norm_host = nullptr;  // pinned, 2 doubles
+    double norm_host[2] = {0, 0};
+    double* lu_scratch = nullptr;  // cluster LU pivot candidates
+    bool own_arena = true;         // false: memory given by the caller
     // mg_guide state (multigrid.hh:34-118)
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;
     double iter_avg = 16, iter_var = 1000000, alpha = 3.0 / 16, tol = 0;

@@ -1,6 +1,8 @@
 // Set-up kernels: Galerkin coarse operators (RAT) and their boxes, and the
 // coarsest-level dense LU.  FP64 throughout.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "layout.cuh"
 
 namespace pgmg {
@@ -37,7 +39,7 @@ __device__ inline AxisList axis_list(int I, int ma) {
 // b_red :1105-1110; b_ex :1276-1283): coarse box = [0,1)^3 extended by the
 // grid_map'ed global box of every fine point that transfers to the coarse
 // point.  One thread per coarse point; boxes as int8[6] natural order.
-__global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGeom gc, const int8_t* __restrict__ Sf,
+static __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGeom gc, const int8_t* __restrict__ Sf,
                                                     int8_t* __restrict__ Sc) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= gc.npts) return;
@@ -69,7 +71,7 @@ __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGeom gc, 
 // by powers of two are exact, sums are rounded one by one (no fused
 // multiply-add), so the result matches the reference bit for bit.
 // Grid: one thread per coarse point.  Output: colour-major coarse stencils.
-__global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
+static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
                                                   const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= gc.npts) return;
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom gc, co
 // ---------------------------------------------------------------------------
 // Coarsest level: dense column-major matrix Aexact[row + col*n] from the
 // level's stencils (region_tr.cc:489-508, non-periodic: no wrap needed).
-__global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, double* __restrict__ M) {
+static __global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, double* __restrict__ M) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long n = g.npts;
     if (q >= n * 27) return;
@@ -162,7 +164,7 @@ __global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, double* __
 // operations as DGETF2 (and the oracle's restatement): pivot = first row of
 // largest |a_ij|, i >= j; swap rows across the whole matrix; scale the
 // sub-column by 1/a_jj.  info[0] = first zero pivot (1-based).  One block.
-__global__ void __launch_bounds__(1024) k_lu_pivot(double* __restrict__ M, int n, int j, int* __restrict__ piv,
+static __global__ void __launch_bounds__(1024) k_lu_pivot(double* __restrict__ M, int n, int j, int* __restrict__ piv,
                                                    int* __restrict__ info) {
     __shared__ double sv[32];
     __shared__ int si[32];
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(1024) k_lu_pivot(double* __restrict__ M, int n
 }
 
 // Rank-1 update of the trailing block after column j.  Thread per element.
-__global__ void __launch_bounds__(256) k_lu_update(double* __restrict__ M, int n, int j) {
+static __global__ void __launch_bounds__(256) k_lu_update(double* __restrict__ M, int n, int j) {
     long rem = n - j - 1;
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= rem * rem) return;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(256) k_lu_update(double* __restrict__ M, int n
 // A x = e_c with the recorded interchanges, unit-lower forward and upper
 // backward substitution (column-oriented, as DGETRS), working in column c
 // of the output so that a warp's accesses are contiguous.
-__global__ void __launch_bounds__(128) k_lu_inverse(const double* __restrict__ M, const int* __restrict__ piv,
+static __global__ void __launch_bounds__(128) k_lu_inverse(const double* __restrict__ M, const int* __restrict__ piv,
                                                     int n, double* __restrict__ Minv) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(128) k_lu_inverse(const double* __restrict__ M
 // warp per row, FP64 accumulation, fixed reduction tree.  r is the level's
 // colour-major source (type T), x its halo'd solution.
 template <class T>
-__global__ void __launch_bounds__(256) k_lu_apply(LevelGeom g, const double* __restrict__ Minv,
+static __global__ void __launch_bounds__(256) k_lu_apply(LevelGeom g, const double* __restrict__ Minv,
                                                   const T* __restrict__ r, T* __restrict__ x) {
     int n = (int)g.npts;
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(256) k_lu_apply(LevelGeom g, const double* __r
 // in parallel -- the same operations as the oracle's restatement, so the
 // result matches it bit for bit.  buf: n doubles of scratch.
 template <class T>
-__global__ void __launch_bounds__(1024) k_lu_solve_exact(LevelGeom g, const double* __restrict__ M,
+static __global__ void __launch_bounds__(1024) k_lu_solve_exact(LevelGeom g, const double* __restrict__ M,
                                                          const int* __restrict__ piv, const T* __restrict__ r,
                                                          T* __restrict__ x, double* __restrict__ b) {
     int n = (int)g.npts;
@@ -317,6 +319,157 @@ __global__ void __launch_bounds__(1024) k_lu_solve_exact(LevelGeom g, const doub
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
         x[g.xi(i, j, k)] = (T)b[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Input synthesis on the device (the host generators of problems.cpp, same
+// operation order, no fused multiply-add, so the results are bit for bit the
+// host arrays):
+//   k_assemble_q1: Q1 FEM stencils of -div(kappa grad u) from a cell field
+//   (kappa itself, or g with kappa = exp(sigma*g) when from_log), Dirichlet
+//   fix rows on the boundary, boxes; written straight into the level-0
+//   colour-major stencils.
+__device__ __forceinline__ double cell_kappa(const double* c, long idx, int from_log, double sigma) {
+    if (!c) return 1.0;
+    return from_log ? exp(sigma * c[idx]) : c[idx];
+}
+
+static __global__ void __launch_bounds__(128) k_assemble_q1(LevelGeom g, const double* __restrict__ cells, int from_log,
+                                                     double sigma, double h, double* __restrict__ A,
+                                                     int8_t* __restrict__ S) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    long nx = g.m - 1, ny = g.n - 1;
+    const double khat[4] = {1.0 / 3.0, 0.0, -1.0 / 12.0, -1.0 / 12.0};
+    double c[27];
+#pragma unroll
+    for (int s = 0; s < 27; s++) c[s] = 0.0;
+    bool interior = i > 0 && i < g.m - 1 && j > 0 && j < g.n - 1 && k > 0 && k < g.o - 1;
+    if (interior) {
+        for (int ce = -1; ce <= 0; ce++)
+            for (int cb = -1; cb <= 0; cb++)
+                for (int ca = -1; ca <= 0; ca++) {
+                    double ke = __dmul_rn(h, cell_kappa(cells, (i + ca) + nx * ((j + cb) + ny * (long)(k + ce)), from_log, sigma));
+                    for (int ee = 0; ee < 2; ee++)
+                        for (int bb = 0; bb < 2; bb++)
+                            for (int aa = 0; aa < 2; aa++) {
+                                int diff = (aa != -ca) + (bb != -cb) + (ee != -ce);
+                                int s = (aa + ca + 1) + 3 * (bb + cb + 1) + 9 * (ee + ce + 1);
+                                c[s] = __dadd_rn(c[s], __dmul_rn(ke, khat[diff]));
+                            }
+                }
+    } else {
+        double sum = 0;
+        int cnt = 0;
+        for (int e = -1; e <= 0; e++)
+            for (int b = -1; b <= 0; b++)
+                for (int a = -1; a <= 0; a++) {
+                    long ci = i + a, cj = j + b, ck = k + e;
+                    if (ci < 0 || cj < 0 || ck < 0 || ci >= nx || cj >= ny || ck >= g.o - 1) continue;
+                    sum = __dadd_rn(sum, cell_kappa(cells, ci + nx * (cj + ny * ck), from_log, sigma));
+                    cnt++;
+                }
+        c[13] = __dmul_rn(__dmul_rn(8.0 / 3.0, h), __ddiv_rn(sum, (double)cnt));
+    }
+#pragma unroll
+    for (int s = 0; s < 27; s++) A[g.ai(i, j, k, s)] = c[s];
+    int8_t* b = S + 6 * q;
+    b[0] = b[2] = b[4] = interior ? -1 : 0;
+    b[1] = b[3] = b[5] = interior ? 2 : 1;
+}
+
+// Right-hand side: interior uniform[-1,1] from SplitMix64(key ^ index), the
+// integer recipe of pgmg_problem_rhs, boundary 0; into the colour-major source.
+__device__ __forceinline__ uint64_t d_splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static __global__ void __launch_bounds__(256) k_rhs_uniform(LevelGeom g, uint64_t seed, double* __restrict__ r) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    uint64_t key = (seed + 0x5851F42D4C957F2Dull) * 0x2545F4914F6CDD1Dull;
+    bool interior = i > 0 && i < g.m - 1 && j > 0 && j < g.n - 1 && k > 0 && k < g.o - 1;
+    double v = 0.0;
+    if (interior) {
+        double u = (double)((d_splitmix64(key ^ (uint64_t)q) >> 11) + 1) * (1.0 / 9007199254740992.0);
+        v = 2.0 * (u - 0.5);
+    }
+    r[g.ri(i, j, k)] = v;
+}
+
+// ---------------------------------------------------------------------------
+// The whole LU factorisation of the coarsest level in one thread-block
+// cluster: per column, pivot search (each CTA's candidate to global scratch,
+// then every thread picks the first largest), row swap, scaling and the
+// rank-1 update, separated by hardware cluster barriers.  Every matrix entry
+// sees exactly the operations of k_lu_pivot / k_lu_update, so the factors are
+// bit for bit those of the per-column launches.  scratch: 2*CTAs doubles.
+__device__ __forceinline__ void lu_better(double v, int i, double& bv, int& bi) {
+    if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+}
+
+static __global__ void __launch_bounds__(512) k_lu_cluster(double* M, int n, int* __restrict__ piv, int* __restrict__ info,
+                                                    double* scratch) {
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    int ncta = (int)cl.num_blocks();
+    int rank = (int)cl.block_rank();
+    int nth = ncta * blockDim.x;
+    int tid = rank * blockDim.x + threadIdx.x;
+    __shared__ double sv[32];
+    __shared__ int si[32];
+    if (tid == 0) info[0] = 0;
+    for (int j = 0; j < n; j++) {
+        double bv = -1.0;
+        int bi = n;
+        for (int i = j + tid; i < n; i += nth) lu_better(fabs(__ldcg(M + i + (long)j * n)), i, bv, bi);
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            lu_better(ov, oi, bv, bi);
+        }
+        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) { sv[w] = bv; si[w] = bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int q = 1; q < (int)(blockDim.x >> 5); q++) lu_better(sv[q], si[q], sv[0], si[0]);
+            scratch[2 * rank] = sv[0];
+            scratch[2 * rank + 1] = (double)si[0];
+        }
+        cl.sync();
+        bv = -1.0;
+        bi = n;
+        for (int c = 0; c < ncta; c++) lu_better(__ldcg(scratch + 2 * c), (int)__ldcg(scratch + 2 * c + 1), bv, bi);
+        int p = bi < n ? bi : j;
+        if (tid == 0) piv[j] = p + 1;
+        double apj = __ldcg(M + p + (long)j * n);
+        if (apj != 0.0) {
+            if (p != j)
+                for (int c = tid; c < n; c += nth) {
+                    double a = __ldcg(M + j + (long)c * n), b2 = __ldcg(M + p + (long)c * n);
+                    M[j + (long)c * n] = b2;
+                    M[p + (long)c * n] = a;
+                }
+            cl.sync();
+            double r = 1.0 / __ldcg(M + j + (long)j * n);
+            for (int i = j + 1 + tid; i < n; i += nth) M[i + (long)j * n] = __dmul_rn(__ldcg(M + i + (long)j * n), r);
+        } else if (tid == 0 && info[0] == 0) {
+            info[0] = j + 1;
+        }
+        cl.sync();
+        long rem = n - j - 1;
+        for (long q = tid; q < rem * rem; q += nth) {
+            int i = j + 1 + (int)(q % rem);
+            int k = j + 1 + (int)(q / rem);
+            double u = __ldcg(M + j + (long)k * n);
+            if (u != 0.0) M[i + (long)k * n] = __dsub_rn(__ldcg(M + i + (long)k * n), __dmul_rn(__ldcg(M + i + (long)j * n), u));
+        }
+        cl.sync();
     }
 }
 

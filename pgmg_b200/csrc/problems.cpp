@@ -76,6 +76,16 @@ extern "C" {
 
 int pgmg_problem_kappa(int m, int n, int o, double sigma, uint64_t seed, double width, double* kappa) {
     if (m < 2 || n < 2 || o < 2 || !kappa) return PGMG_ERR_ARG;
+    int st = pgmg_problem_gauss(m, n, o, seed, width, kappa);
+    if (st) return st;
+    long nc = (long)(m - 1) * (n - 1) * (o - 1);
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nc; c++) kappa[c] = std::exp(sigma * kappa[c]);
+    return PGMG_OK;
+}
+
+int pgmg_problem_gauss(int m, int n, int o, uint64_t seed, double width, double* out) {
+    if (m < 2 || n < 2 || o < 2 || !out) return PGMG_ERR_ARG;
     long nx = m - 1, ny = n - 1, nz = o - 1, nc = nx * ny * nz;
     std::vector<double> g(nc);
 #pragma omp parallel for schedule(static)
@@ -117,7 +127,7 @@ int pgmg_problem_kappa(int m, int n, int o, double sigma, uint64_t seed, double 
     var /= (double)nc;
     double inv_sd = var > 0 ? 1.0 / std::sqrt(var) : 0.0;
 #pragma omp parallel for schedule(static)
-    for (long c = 0; c < nc; c++) kappa[c] = std::exp(sigma * (g[c] - mean) * inv_sd);
+    for (long c = 0; c < nc; c++) out[c] = (g[c] - mean) * inv_sd;
     return PGMG_OK;
 }
 
