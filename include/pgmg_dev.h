@@ -268,6 +268,19 @@ pgmg_status pgmg_batch_attach(pgmg_batch *b, int slot, pgmg_handle *h);
 pgmg_status pgmg_batch_detach(pgmg_batch *b, int slot);
 pgmg_status pgmg_batch_solve(pgmg_batch *b, double tol, int max_cycles, int *cycles, double *relres);
 pgmg_status pgmg_batch_launch_count(pgmg_batch *b, long long *n);
+/* Step-level control for continuous batching: pgmg_batch_begin starts a
+ * solve from x = 0 in an attached slot (after its handle's set-up and source
+ * are complete); pgmg_batch_step runs one refinement step (residual and
+ * convergence check, then a V-cycle) for every running slot and returns how
+ * many still run; pgmg_batch_poll reads the per-slot flags, cycle counts and
+ * relative residuals (arrays of max_slots, each may be NULL).  Slots may be
+ * attached, begun and detached between steps; a batch shape that persists is
+ * replayed as a captured CUDA graph (pgmg_batch_set_graphs(b, 0) turns that
+ * off). */
+pgmg_status pgmg_batch_begin(pgmg_batch *b, int slot);
+pgmg_status pgmg_batch_step(pgmg_batch *b, double tol, int max_cycles, int *n_active);
+pgmg_status pgmg_batch_poll(pgmg_batch *b, int *active, int *cycles, double *relres);
+pgmg_status pgmg_batch_set_graphs(pgmg_batch *b, int on);
 
 /* ---- host problem generators (no GPU needed) ---------------------------- */
 

@@ -97,6 +97,10 @@ SIGNATURES = [
     ("pgmg_batch_detach", C.c_int, [_VP, C.c_int]),
     ("pgmg_batch_solve", C.c_int, [_VP, C.c_double, C.c_int, _VP, _VP]),
     ("pgmg_batch_launch_count", C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    ("pgmg_batch_begin", C.c_int, [_VP, C.c_int]),
+    ("pgmg_batch_step", C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int)]),
+    ("pgmg_batch_poll", C.c_int, [_VP, _VP, _VP, _VP]),
+    ("pgmg_batch_set_graphs", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_create_in", C.c_int, [C.POINTER(Dims), _VP, C.c_size_t, C.POINTER(C.c_void_p)]),
     ("pgmg_dev_assemble_q1", C.c_int, [_VP, _VP, C.c_int, C.c_double]),
     ("pgmg_dev_rhs_uniform", C.c_int, [_VP, C.c_uint64]),
@@ -452,6 +456,24 @@ class Batch:
         rr = np.zeros(self.max_slots)
         self._ck(lib().pgmg_batch_solve(self._b, tol, max_cycles, _ptr(cyc), _ptr(rr)), "batch_solve")
         return cyc, rr
+
+    def begin(self, slot: int):
+        self._ck(lib().pgmg_batch_begin(self._b, slot), "batch_begin")
+
+    def step(self, tol: float = 1e-10, max_cycles: int = 100) -> int:
+        n = C.c_int()
+        self._ck(lib().pgmg_batch_step(self._b, tol, max_cycles, C.byref(n)), "batch_step")
+        return n.value
+
+    def poll(self):
+        act = np.zeros(self.max_slots, np.int32)
+        cyc = np.zeros(self.max_slots, np.int32)
+        rr = np.zeros(self.max_slots)
+        self._ck(lib().pgmg_batch_poll(self._b, _ptr(act), _ptr(cyc), _ptr(rr)), "batch_poll")
+        return act, cyc, rr
+
+    def set_graphs(self, on: bool):
+        self._ck(lib().pgmg_batch_set_graphs(self._b, int(on)), "batch_set_graphs")
 
     @property
     def launches(self) -> int:

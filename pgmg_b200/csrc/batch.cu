@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kBlock) kb_interp(const BSlot<T>* __restrict__
 // stores it as the FP32 correction source when TO = float.
 template <class T, class TO>
 __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
-                                                   const int* __restrict__ active, int x_is_zero) {
+                                                   const int* __restrict__ active, const int* __restrict__ first) {
     __shared__ double sh[64];
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ 
     long p = (lb % nb) * blockDim.x + threadIdx.x;
     TO* out = std::is_same<TO, float>::value ? reinterpret_cast<TO*>(B.r[0]) : nullptr;
     double a = 0, b = 0;
-    if (x_is_zero) {
+    if (first[s]) {
         if (p < nc) {
             double rv = B.r64[(long)col * g.Nc + p];
             if (out) out[(long)col * g.Nc + p] = (TO)rv;
@@ -160,8 +160,9 @@ __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ 
 // count the cycle that is about to run.
 template <class T>
 __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
-                                                  int* __restrict__ active, int* __restrict__ cycles,
-                                                  double* __restrict__ relres, double tol, int max_cycles) {
+                                                  int* __restrict__ active, int* __restrict__ first,
+                                                  int* __restrict__ cycles, double* __restrict__ relres,
+                                                  double tol, int max_cycles) {
     __shared__ double sh[64];
     int s = M->slot[blockIdx.x];
     if (!active[s]) return;
@@ -177,6 +178,7 @@ __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S
     if (threadIdx.x == 0) {
         double rr = b > 0 ? sqrt(a / b) : sqrt(a);
         relres[s] = rr;
+        first[s] = 0;
         if (isnan(rr) || rr < tol || cycles[s] >= max_cycles) active[s] = 0;
         else cycles[s]++;
     }
@@ -219,13 +221,29 @@ __global__ void __launch_bounds__(kBlock) kb_clear64(const BSlot<double>* S64, c
     x64[g.xi(i, j, k)] = 0.0;
 }
 
-__global__ void kb_reset(const BMap* __restrict__ M, int* active, int* cycles, double* relres) {
+__global__ void kb_reset(const BMap* __restrict__ M, int* active, int* first, int* cycles, double* relres) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M->n) return;
     int s = M->slot[e];
     active[s] = 1;
+    first[s] = 1;
     cycles[s] = 0;
     relres[s] = 0;
+}
+
+// Starts one slot: x = 0 on its level 0 and fresh flags.
+__global__ void __launch_bounds__(kBlock) kb_begin(LevelGeom g, double* x64, int s, int* active, int* first,
+                                                   int* cycles, double* relres) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q == 0) {
+        active[s] = 1;
+        first[s] = 1;
+        cycles[s] = 0;
+        relres[s] = 0;
+    }
+    if (q >= g.npts) return;
+    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    x64[g.xi(i, j, k)] = 0.0;
 }
 
 }  // namespace
@@ -242,6 +260,7 @@ struct pgmg_batch {
     BMap* maps = nullptr;        // built per shape
     int nmaps_cap = 0;
     int* active = nullptr;
+    int* first = nullptr;
     int* cycles = nullptr;
     double* relres = nullptr;
     int* cluster_slots = nullptr;
@@ -252,7 +271,9 @@ struct pgmg_batch {
     std::vector<BMap> hmaps;
     int map_gs[kMaxLv], map_res[kMaxLv], map_rst[kMaxLv], map_int[kMaxLv], map_chk = -1, map_pt0 = -1, map_red = -1;
     int v_down = 2, v_up = 2;
-    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};  // [first step (x = 0), later steps]
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};  // one captured step (index 0 used)
+    int stable_steps = 0;  // steps run since the last shape change (capture from the second)
+    bool use_graphs = true;
     double cap_tol = -1;  // tol and cycle cap the step graphs were captured with
     int cap_max = -1;
     long long launches = 0;
@@ -407,14 +428,14 @@ pgmg_status build_shape(pgmg_batch* b) {
     } while (0)
 
 template <class T>
-pgmg_status enqueue_step(pgmg_batch* b, int first, double tol, int max_cycles) {
+pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
     const BSlot<T>* S = static_cast<const BSlot<T>*>(b->slot_table);
     auto M = [&](int m) { return b->maps + m; };
     using TO = T;
-    kb_check<T, TO><<<map_blocks(b, b->map_chk), kBlock, 0, b->stream>>>(S, M(b->map_chk), b->active, first);
+    kb_check<T, TO><<<map_blocks(b, b->map_chk), kBlock, 0, b->stream>>>(S, M(b->map_chk), b->active, b->first);
     BKL();
-    kb_reduce<T><<<(int)b->members.size(), 1024, 0, b->stream>>>(S, M(b->map_red), b->active, b->cycles, b->relres,
-                                                                  tol, max_cycles);
+    kb_reduce<T><<<(int)b->members.size(), 1024, 0, b->stream>>>(S, M(b->map_red), b->active, b->first, b->cycles,
+                                                                  b->relres, tol, max_cycles);
     BKL();
     if (std::is_same<T, float>::value) {
         kb_clear32<<<map_blocks(b, b->map_pt0), kBlock, 0, b->stream>>>(
@@ -470,11 +491,23 @@ pgmg_status enqueue_step(pgmg_batch* b, int first, double tol, int max_cycles) {
 }
 
 template <class T>
-pgmg_status run_step(pgmg_batch* b, int first, double tol, int max_cycles) {
-    cudaGraphExec_t& ex = b->step_graph[first ? 0 : 1];
+pgmg_status run_step(pgmg_batch* b, double tol, int max_cycles) {
+    // tol and the cycle cap are graph parameters: recapture if they change.
+    if (tol != b->cap_tol || max_cycles != b->cap_max) {
+        drop_step_graphs(b);
+        b->cap_tol = tol;
+        b->cap_max = max_cycles;
+    }
+    // A new shape runs its first step with plain launches; a shape that
+    // persists is captured once and replayed.
+    if (!b->use_graphs || b->stable_steps < 1) {
+        b->stable_steps++;
+        return enqueue_step<T>(b, tol, max_cycles);
+    }
+    cudaGraphExec_t& ex = b->step_graph[0];
     if (!ex) {
         BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        pgmg_status st = enqueue_step<T>(b, first, tol, max_cycles);
+        pgmg_status st = enqueue_step<T>(b, tol, max_cycles);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
         if (st != PGMG_OK) {
@@ -490,21 +523,39 @@ pgmg_status run_step(pgmg_batch* b, int first, double tol, int max_cycles) {
         }
     }
     BCK(cudaGraphLaunch(ex, b->stream));
+    b->stable_steps++;
+    return PGMG_OK;
+}
+
+template <class T>
+pgmg_status batch_step(pgmg_batch* b, double tol, int max_cycles, int* n_active) {
+    if (b->dirty) {
+        BTRY(build_shape<T>(b));
+        b->stable_steps = 0;
+    }
+    if (b->members.empty()) {
+        if (n_active) *n_active = 0;
+        return PGMG_OK;
+    }
+    BTRY(run_step<T>(b, tol, max_cycles));
+    std::vector<int> act(kMaxSlots);
+    BCK(cudaMemcpyAsync(act.data(), b->active, sizeof(int) * kMaxSlots, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    int na = 0;
+    for (int s : b->members) na += act[s] ? 1 : 0;
+    if (n_active) *n_active = na;
     return PGMG_OK;
 }
 
 template <class T>
 pgmg_status batch_solve(pgmg_batch* b, double tol, int max_cycles, int* cycles, double* relres) {
-    if (b->dirty) BTRY(build_shape<T>(b));
-    if (b->members.empty()) return PGMG_OK;
-    // tol and the cycle cap are graph parameters: recapture if they change.
-    if (tol != b->cap_tol || max_cycles != b->cap_max) {
-        drop_step_graphs(b);
-        b->cap_tol = tol;
-        b->cap_max = max_cycles;
+    if (b->dirty) {
+        BTRY(build_shape<T>(b));
+        b->stable_steps = 0;
     }
+    if (b->members.empty()) return PGMG_OK;
     int nm = (int)b->members.size();
-    kb_reset<<<(nm + 127) / 128, 128, 0, b->stream>>>(b->maps + b->map_red, b->active, b->cycles, b->relres);
+    kb_reset<<<(nm + 127) / 128, 128, 0, b->stream>>>(b->maps + b->map_red, b->active, b->first, b->cycles, b->relres);
     BKL();
     kb_clear64<<<map_blocks(b, b->map_pt0), kBlock, 0, b->stream>>>(
         std::is_same<T, double>::value ? static_cast<const BSlot<double>*>(b->slot_table) : nullptr,
@@ -512,14 +563,10 @@ pgmg_status batch_solve(pgmg_batch* b, double tol, int max_cycles, int* cycles, 
         b->maps + b->map_pt0);
     BKL();
     for (int s : b->members) b->slots[s]->x0_zero = false;
-    std::vector<int> act(kMaxSlots);
     for (int step = 0; step <= max_cycles; step++) {
-        BTRY(run_step<T>(b, step == 0, tol, max_cycles));
-        BCK(cudaMemcpyAsync(act.data(), b->active, sizeof(int) * kMaxSlots, cudaMemcpyDeviceToHost, b->stream));
-        BCK(cudaStreamSynchronize(b->stream));
-        bool any = false;
-        for (int s : b->members) any = any || act[s];
-        if (!any) break;
+        int na = 0;
+        BTRY(batch_step<T>(b, tol, max_cycles, &na));
+        if (!na) break;
     }
     std::vector<int> cyc(kMaxSlots);
     std::vector<double> rr(kMaxSlots);
@@ -557,6 +604,7 @@ pgmg_status pgmg_batch_create(int max_slots, int precision, int device, pgmg_bat
         cudaMalloc(&b->slot_table, tb * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->plan_table, pb * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->active, sizeof(int) * kMaxSlots) != cudaSuccess ||
+        cudaMalloc(&b->first, sizeof(int) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->cycles, sizeof(int) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->relres, sizeof(double) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->cluster_slots, sizeof(int) * kMaxSlots) != cudaSuccess) {
@@ -565,6 +613,7 @@ pgmg_status pgmg_batch_create(int max_slots, int precision, int device, pgmg_bat
         return PGMG_ERR_MEMORY;
     }
     cudaMemsetAsync(b->active, 0, sizeof(int) * kMaxSlots, b->stream);
+    cudaMemsetAsync(b->first, 0, sizeof(int) * kMaxSlots, b->stream);
     cudaMemsetAsync(b->cycles, 0, sizeof(int) * kMaxSlots, b->stream);
     cudaStreamSynchronize(b->stream);
     *out = b;
@@ -579,6 +628,7 @@ pgmg_status pgmg_batch_destroy(pgmg_batch* b) {
     cudaFree(b->plan_table);
     cudaFree(b->maps);
     cudaFree(b->active);
+    cudaFree(b->first);
     cudaFree(b->cycles);
     cudaFree(b->relres);
     cudaFree(b->cluster_slots);
@@ -610,8 +660,43 @@ pgmg_status pgmg_batch_attach(pgmg_batch* b, int slot, pgmg_handle* h) {
 
 pgmg_status pgmg_batch_detach(pgmg_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->slots.size()) return PGMG_ERR_ARG;
+    BCK(cudaMemsetAsync(b->active + slot, 0, sizeof(int), b->stream));
     b->slots[slot] = nullptr;
     b->dirty = true;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_batch_begin(pgmg_batch* b, int slot) {
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return PGMG_ERR_ARG;
+    pgmg_handle* h = b->slots[slot];
+    BCK(cudaStreamSynchronize(h->stream));  // its set-up and source are complete
+    const LevelGeom& g = h->L[0].g;
+    kb_begin<<<nblk(g.npts), kBlock, 0, b->stream>>>(g, h->L[0].x64, slot, b->active, b->first, b->cycles, b->relres);
+    BKL();
+    h->x0_zero = false;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_batch_step(pgmg_batch* b, double tol, int max_cycles, int* n_active) {
+    if (!b || max_cycles < 0) return PGMG_ERR_ARG;
+    if (b->precision == PGMG_MIXED) return batch_step<float>(b, tol, max_cycles, n_active);
+    return batch_step<double>(b, tol, max_cycles, n_active);
+}
+
+pgmg_status pgmg_batch_poll(pgmg_batch* b, int* active, int* cycles, double* relres) {
+    if (!b) return PGMG_ERR_ARG;
+    size_t ns = b->slots.size();
+    if (active) BCK(cudaMemcpyAsync(active, b->active, sizeof(int) * ns, cudaMemcpyDeviceToHost, b->stream));
+    if (cycles) BCK(cudaMemcpyAsync(cycles, b->cycles, sizeof(int) * ns, cudaMemcpyDeviceToHost, b->stream));
+    if (relres) BCK(cudaMemcpyAsync(relres, b->relres, sizeof(double) * ns, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_batch_set_graphs(pgmg_batch* b, int on) {
+    if (!b) return PGMG_ERR_ARG;
+    drop_step_graphs(b);
+    b->use_graphs = on != 0;
     return PGMG_OK;
 }
 

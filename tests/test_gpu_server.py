@@ -1,0 +1,39 @@
+"""Continuous-batching server: every request's result equals the same problem
+solved alone (bit for bit), under staggered arrivals, RHS-only reuse of
+resident hierarchies, and eviction under a small memory cap."""
+import numpy as np
+import pytest
+
+import pgmg_b200 as P
+from pgmg_b200.server import FieldPool, SolveServer, poisson_requests
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(req, fields):
+    m, n, o = req.shape
+    G = P.Multigrid(m, n, o, precision=P.MIXED)
+    G.assemble_q1(fields.get(req.shape, req.field).data_ptr(), from_log=True, sigma=req.sigma)
+    G.rhs_uniform(req.rhs_seed)
+    G.clear_x(0)
+    cyc, rr = G.solve(1e-10, 100, 1)
+    x = G.get_x(0)
+    G.close()
+    return cyc, rr, x
+
+
+@pytest.mark.parametrize("cap_mb", [2000, 40])
+def test_server_results_equal_alone(cap_mb):
+    reqs = poisson_requests(rate=120.0, duration=0.25, seed=3, reuse=0.3, sizes=(17, 33), sigma=(0.5, 2.0))
+    assert len(reqs) >= 10
+    fields = FieldPool(0)
+    srv = SolveServer(cap_mb * 1e6, max_slots=8, precision=P.MIXED, keep_solutions=True, fields=fields)
+    done = srv.run(reqs)
+    assert len(done) == len(reqs)
+    assert any(r.reused for r in done)
+    for r in done:
+        assert r.relres < 1e-10 and r.finished >= r.arrival
+        cyc, rr, x = alone(r, fields)
+        assert cyc == r.cycles and rr == r.relres
+        assert np.array_equal(x, r.x), r.rid
+    srv.close()
