@@ -51,6 +51,13 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--workload", default="solve257",
+                    choices=["solve257", "small65", "large513", "batch96", "serve"],
+                    help="solve257 is the benchmark line; the others measure the other configurations")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="only the mixed-precision solves of the benchmark problem (for profiler launch lists)")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     return ap.parse_args()
 
 
@@ -386,10 +393,281 @@ def cpu_baseline(a, coef, S, r, G):
                       f"lu_enabled={lu})"}
 
 
+# ----------------------------------------------------------------- other configurations
+
+def vcycle_bytes(dims, s, v_down=2, v_up=2):
+    """Algorithmic bytes of one V-cycle (2+l / 1+l+... sweeps as the cycle runs)
+    with s-byte scalars: sweeps (27+3)s per point, residual+restriction
+    (27+2)s per fine point + s per coarse point, interpolation 2s per fine point
+    + s per coarse point, coarse solve n^2 * 8."""
+    npts = [m * n * o for (m, n, o) in dims]
+    b = 0.0
+    L = len(dims)
+    for l in range(L - 1):
+        b += (v_down + l) * 30 * s * npts[l] + (v_up + l) * 30 * s * npts[l]
+        b += 29 * s * npts[l] + s * npts[l + 1]
+        b += 2 * s * npts[l] + s * npts[l + 1]
+    b += npts[-1] ** 2 * 8
+    return b
+
+
+def level_dims(m, n, o):
+    dims = [(m, n, o)]
+    while m * n * o > 1024:
+        m, n, o = (m + 2) >> 1, (n + 2) >> 1, (o + 2) >> 1
+        dims.append((m, n, o))
+    return dims
+
+
+def ir_step_bytes(m, n, o):
+    """One mixed-precision refinement step: FP64 residual (27+2)*8 + FP32 source
+    write 4, FP32 V-cycle, FP32 clear 4 and FP64 update 8+4+8 per fine point."""
+    N = m * n * o
+    return vcycle_bytes(level_dims(m, n, o), 4) + (29 * 8 + 4 + 4 + 20) * N
+
+
+def timed(stream, fn, reps):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    out = None
+    for _ in range(reps):
+        out = fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps / 1e3, out
+
+
+def run_small65(a):
+    """Config 1: 65^3 constant-coefficient Q1, Dirichlet, FP64, to 1e-10;
+    this library on the GPU and the reference on one host core."""
+    import torch
+
+    import pgmg_b200 as P
+    from oracle.pyoracle import Reference, ref_available
+    m = 65
+    coef, S = P.problem_q1(m, m, m)
+    r = P.problem_rhs(m, m, m, a.seed)
+    st = torch.cuda.Stream()
+    G = P.Multigrid(m, m, m)
+    G.set_stream(st.cuda_stream)
+    G.setup_matrices(coef, S)
+    G.setup_fields(r)
+
+    def solve():
+        G.clear_x(0)
+        return G.solve(a.tol, 100, 0)
+    for _ in range(a.warmup):
+        solve()
+    t, (cyc, rr) = timed(st, solve, a.steps)
+    ref = None
+    if ref_available():
+        R = Reference(m, m, m, S, coef, r)
+        ts = []
+        for _ in range(3):
+            R.set_x(0, np.zeros(m ** 3))
+            t0 = time.perf_counter()
+            n_ref, rr_ref = reference_cycles(R, a.tol)
+            ts.append(time.perf_counter() - t0)
+        ref = {"value": float(np.median(ts)), "unit": UNIT, "cores": 1, "kind": "reference", "cycles": n_ref,
+               "lu_enabled": R.lu_enabled, "sample": "3 full solves, median"}
+    print(json.dumps({"workload": "65^3 constant-kappa Q1 FP64 to 1e-10 (config 1)", "value": t, "unit": UNIT,
+                      "cycles": cyc, "relres": rr, "steps": a.steps, "warmup": a.warmup, "cpu_baseline": ref}))
+
+
+def run_large513(a):
+    """Config 3: 513^3, sigma 2.3: FP64 and mixed solves to 1e-10, and the
+    error of each against an FP64 solve driven to 1e-13."""
+    import torch
+
+    import pgmg_b200 as P
+    m = 513
+    sigma = 2.3
+    t0 = time.perf_counter()
+    g = P.problem_gauss(m, m, m, a.seed, 8.0)
+    gen_s = time.perf_counter() - t0
+    st = torch.cuda.Stream()
+    out = {"workload": "513^3 Q1 variable-kappa sigma=2.3 to 1e-10 (config 3)", "unit": UNIT,
+           "host_generation_s": gen_s}
+    xs = {}
+    for name, prec in (("fp64", P.FP64), ("mixed", P.MIXED)):
+        G = P.Multigrid(m, m, m, precision=prec)
+        G.set_stream(st.cuda_stream)
+        t0 = time.perf_counter()
+        G.assemble_q1(g, from_log=True, sigma=sigma)
+        G.sync()
+        setup = time.perf_counter() - t0
+        G.rhs_uniform(a.seed)
+
+        def solve():
+            G.clear_x(0)
+            return G.solve(a.tol, 200, 0)
+        for _ in range(max(1, a.warmup - 1)):
+            solve()
+        t, (cyc, rr) = timed(st, solve, max(1, a.steps // 2))
+        xs[name] = G.get_x(0)
+        out[name] = {"value": t, "cycles": cyc, "relres": rr, "setup_s": setup, "memory_gb": G.memory_bytes / 1e9}
+        if prec == P.FP64:
+            # reference solution: continue the FP64 iteration to 1e-13
+            cyc2, rr2 = G.solve(1e-13, 300, 1)
+            xs["ref"] = G.get_x(0)
+            out["reference_solution"] = {"relres": rr2, "extra_cycles": cyc2}
+        G.close()
+        torch.cuda.empty_cache()
+    nrm = np.abs(xs["ref"]).max()
+    out["fp64"]["max_err_vs_1e-13"] = float(np.abs(xs["fp64"] - xs["ref"]).max() / nrm)
+    out["mixed"]["max_err_vs_1e-13"] = float(np.abs(xs["mixed"] - xs["ref"]).max() / nrm)
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["value"] / out["mixed"]["value"]
+    dims = level_dims(m, m, m)
+    out["fp64"]["vcycle_roofline_ms"] = vcycle_bytes(dims, 8) / measured_peak_hbm()[0] / 1e6
+    print(json.dumps(out))
+
+
+def run_batch96(a):
+    """Config 4: 96 independent problems, dims per axis from {33,65,129},
+    sigma uniform in [0.5,2], mixed precision to 1e-10, one launch per level
+    and colour across all problems, graph-captured steps."""
+    import torch
+
+    import pgmg_b200 as P
+    rng = np.random.default_rng(a.seed)
+    shapes = [tuple(int(v) for v in rng.choice([33, 65, 129], 3)) for _ in range(96)]
+    sigmas = rng.uniform(0.5, 2.0, 96)
+    hs = []
+    t0 = time.perf_counter()
+    for p, (shape, sg) in enumerate(zip(shapes, sigmas)):
+        g = P.problem_gauss(*shape, seed=a.seed * 1000 + p, width=8.0)
+        G = P.Multigrid(*shape, precision=P.MIXED)
+        G.assemble_q1(g, from_log=True, sigma=float(sg))
+        G.rhs_uniform(p)
+        hs.append(G)
+    setup_s = time.perf_counter() - t0
+    B = P.Batch(96, P.MIXED)
+    for p, G in enumerate(hs):
+        B.attach(p, G)
+    for _ in range(a.warmup):
+        cyc, rr = B.solve(a.tol, 100)
+    l0 = B.launches
+    t_b, (cyc, rr) = timed(B_stream := torch.cuda.current_stream(), lambda: B.solve(a.tol, 100), a.steps)
+    launches = (B.launches - l0) // a.steps
+    # wall clock agrees with the device here (the batch syncs each step); use it as well
+    t0 = time.perf_counter()
+    B.solve(a.tol, 100)
+    wall = time.perf_counter() - t0
+    t_batch = max(t_b, wall)
+    # sequential: each problem alone, one after the other
+    st = torch.cuda.Stream()
+    for G in hs:
+        G.set_stream(st.cuda_stream)
+
+    def seq():
+        for G in hs:
+            G.clear_x(0)
+            G.solve(a.tol, 100, 0)
+    seq()
+    t_seq, _ = timed(st, seq, 1)
+    alg = sum(int(c) * ir_step_bytes(*s) for c, s in zip(cyc[:96], shapes))
+    peak, kind = measured_peak_hbm()
+    print(json.dumps({
+        "workload": "96 problems, dims per axis in {33,65,129}, mixed FP32/FP64 to 1e-10 (config 4)",
+        "metric": "solves/s", "value": 96 / t_batch, "unit": "solves/s", "ms_per_batch": t_batch * 1e3,
+        "sequential": {"value": 96 / t_seq, "unit": "solves/s", "ms": t_seq * 1e3},
+        "speedup_vs_sequential": t_seq / t_batch, "max_relres": float(rr[:96].max()),
+        "cycles_min_max": [int(cyc[:96].min()), int(cyc[:96].max())], "gpu_launches_per_batch": launches,
+        "points_total": int(sum(x * y * z for x, y, z in shapes)), "setup_s_all": setup_s,
+        "roofline": {"bound": "hbm", "achieved": alg / t_batch / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / t_batch / 1e9 / peak, "peak_source": kind},
+    }))
+
+
+def run_serve(a):
+    """Config 5: open-loop Poisson arrivals, dims per axis 65..257 rounded to
+    {65,129,257}, sigma in [0.5,2.3], 20% RHS-only reuse, 150 GB cap; solves/s
+    and latency percentiles, next to the same requests served one at a time."""
+    import torch
+
+    import pgmg_b200 as P
+    from pgmg_b200.server import FieldPool, SolveServer, poisson_requests
+    reqs = poisson_requests(a.serve_rate, a.serve_seconds, seed=a.seed, reuse=0.2, sizes=(65, 129, 257),
+                            sigma=(0.5, 2.3))
+    fields = FieldPool(0)
+    for r in reqs:  # the field pool is the requests' payload: generate it before the clock starts
+        fields.get(r.shape, r.field)
+    srv = SolveServer(150e9, max_slots=64, precision=P.MIXED, fields=fields)
+    t0 = time.perf_counter()
+    done = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    lat = np.array([r.latency for r in done])
+    span = max(r.finished for r in done) - min(r.arrival for r in done)
+    out = {"workload": f"serving: Poisson {a.serve_rate:g} req/s for {a.serve_seconds:g} s, dims per axis "
+                       "65..257 -> {65,129,257}, 20% RHS-only reuse, 150 GB cap, mixed to 1e-10 (config 5)",
+           "metric": "solves/s", "value": len(done) / span, "unit": "solves/s", "requests": len(done),
+           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+           "reused": int(sum(r.reused for r in done)), "max_relres": float(max(r.relres for r in done)),
+           "steps": srv.steps, "wall_s": wall}
+    srv.close()
+    del srv
+    torch.cuda.empty_cache()
+    # The same requests one at a time (set-up when not resident, then a solve).
+    cache = {}
+    t0 = time.perf_counter()
+    for r in reqs:
+        G = cache.get(r.problem)
+        if G is None:
+            G = P.Multigrid(*r.shape, precision=P.MIXED)
+            G.assemble_q1(fields.get(r.shape, r.field).data_ptr(), from_log=True, sigma=r.sigma)
+            cache[r.problem] = G
+            total = sum(x.memory_bytes for x in cache.values())
+            while total > 150e9 and len(cache) > 1:
+                k = next(iter(cache))
+                cache.pop(k).close()
+                total = sum(x.memory_bytes for x in cache.values())
+        G.rhs_uniform(r.rhs_seed)
+        G.clear_x(0)
+        G.solve(1e-10, 100, 0)
+    seq = time.perf_counter() - t0
+    out["sequential"] = {"value": len(reqs) / seq, "unit": "solves/s", "s": seq}
+    out["speedup_vs_sequential"] = out["value"] / out["sequential"]["value"]
+    print(json.dumps(out))
+
+
+def run_profile_mixed(a):
+    import torch
+
+    import pgmg_b200 as P
+    m = a.size
+    coef, S, r = build_problem(m, a.sigma, a.seed)
+    st = torch.cuda.Stream()
+    G = P.Multigrid(m, m, m, precision=P.MIXED)
+    G.set_stream(st.cuda_stream)
+    G.setup_matrices(coef, S)
+    G.setup_fields(r)
+    del coef, S
+
+    def solve():
+        G.clear_x(0)
+        return G.solve(a.tol, 100, 0)
+    for _ in range(a.warmup):
+        solve()
+    t, (cyc, rr) = timed(st, solve, a.steps)
+    print(json.dumps({"workload": "mixed only", "value": t, "cycles": cyc, "relres": rr}))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "small65":
+        run_small65(a)
+    elif a.workload == "large513":
+        run_large513(a)
+    elif a.workload == "batch96":
+        run_batch96(a)
+    elif a.workload == "serve":
+        run_serve(a)
+    elif a.profile_mixed:
+        run_profile_mixed(a)
     else:
         run_ours(a)
 

@@ -128,7 +128,8 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
 /* Execution options (tuning; results do not depend on them unless noted).
  *   PGMG_OPT_GRAPHS         1 = replay each V-cycle as a captured CUDA graph (default)
  *   PGMG_OPT_CLUSTER_FIRST  first level run by the one-cluster coarse cycle
- *                           (default: the first level of <= 50000 points;
+ *                           (default: the first level of <= 50000 points,
+ *                           <= 10000 for PGMG_MIXED handles;
  *                           = number of levels disables it)
  *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 16, 8, or 0 (off)
  *   PGMG_OPT_SLAB_BUDGET    bytes of solution vector per z-slab of the 8-colour

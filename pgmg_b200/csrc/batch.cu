@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(kBlock) kb_clear32(const BSlot<float>* __restr
     const LevelGeom& g = S[s].g[0];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     S[s].x[0][g.xi(i, j, k)] = 0.0f;
 }
 
@@ -204,7 +205,8 @@ __global__ void __launch_bounds__(kBlock) kb_add32(const BSlot<float>* __restric
     const LevelGeom& g = S[s].g[0];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     long c = g.xi(i, j, k);
     S[s].x64[c] = S[s].x64[c] + (double)S[s].x[0][c];
 }
@@ -217,7 +219,8 @@ __global__ void __launch_bounds__(kBlock) kb_clear64(const BSlot<double>* S64, c
     double* x64 = S64 ? S64[s].x64 : S32[s].x64;
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     x64[g.xi(i, j, k)] = 0.0;
 }
 
@@ -242,7 +245,8 @@ __global__ void __launch_bounds__(kBlock) kb_begin(LevelGeom g, double* x64, int
         relres[s] = 0;
     }
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     x64[g.xi(i, j, k)] = 0.0;
 }
 
@@ -273,6 +277,7 @@ struct pgmg_batch {
     int v_down = 2, v_up = 2;
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};  // one captured step (index 0 used)
     int stable_steps = 0;  // steps run since the last shape change (capture from the second)
+    long long graph_nodes = 0;  // kernels in the captured step
     bool use_graphs = true;
     double cap_tol = -1;  // tol and cycle cap the step graphs were captured with
     int cap_max = -1;
@@ -506,8 +511,11 @@ pgmg_status run_step(pgmg_batch* b, double tol, int max_cycles) {
     }
     cudaGraphExec_t& ex = b->step_graph[0];
     if (!ex) {
+        long long before = b->launches;
         BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         pgmg_status st = enqueue_step<T>(b, tol, max_cycles);
+        b->graph_nodes = b->launches - before;
+        b->launches = before;
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
         if (st != PGMG_OK) {
@@ -523,6 +531,7 @@ pgmg_status run_step(pgmg_batch* b, double tol, int max_cycles) {
         }
     }
     BCK(cudaGraphLaunch(ex, b->stream));
+    b->launches += b->graph_nodes;
     b->stable_steps++;
     return PGMG_OK;
 }

@@ -568,8 +568,9 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
         }
     }
     h->coarse_first = h->nl - 1;
+    long cmax = dims->precision == PGMG_MIXED ? kClusterMax32 : kClusterMax;
     for (int l = 0; l < h->nl; l++)
-        if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
+        if (h->L[l].g.npts <= cmax) { h->coarse_first = l; break; }
     if (cudaMemsetAsync(h->arena.base, 0, bytes, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         pgmg_dev_destroy(h);

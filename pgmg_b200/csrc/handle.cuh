@@ -14,7 +14,8 @@ constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
 constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
 constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
 constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
-constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
+constexpr long kClusterMax = 50000;   // FP64 V-cycle: levels up to this size run in the one-cluster coarse cycle
+constexpr long kClusterMax32 = 10000; // FP32 V-cycle (mixed handles): the same, measured lower break-even
 constexpr int kClusterThreads = 512;
 
 struct Level {

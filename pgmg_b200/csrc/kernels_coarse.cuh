@@ -43,10 +43,8 @@ template <class T>
 __device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, const T* A, int col, long p0, long p1,
                                          int tid, int nth) {
     for (long p = p0 + tid; p < p1; p += nth) {
-        int i2 = (int)(p % g.M2);
-        long t = p / g.M2;
-        int j2 = (int)(t % g.N2);
-        int k2 = (int)(t / g.N2);
+        int i2, j2, k2;
+        decode_colour(g, p, i2, j2, k2);
         int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
         if (i >= g.m || j >= g.n || k >= g.o) continue;
         long xc = g.xi(i, j, k);
@@ -85,10 +83,8 @@ __device__ __forceinline__ void c_residual(const LevelGeom& g, const T* x, const
     for (long pp = tid; pp < 8 * nc; pp += nth) {
         int col = (int)(pp / nc);
         long p = pp % nc;
-        int i2 = (int)(p % g.M2);
-        long t = p / g.M2;
-        int j2 = (int)(t % g.N2);
-        int k2 = (int)(t / g.N2);
+        int i2, j2, k2;
+        decode_colour(g, p, i2, j2, k2);
         int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
         if (i >= g.m || j >= g.n || k >= g.o) continue;
         long xc = g.xi(i, j, k);
@@ -106,10 +102,8 @@ __device__ __forceinline__ void c_restrict(const LevelGeom& gf, const LevelGeom&
                                            int tid, int nth) {
     int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
     for (long q = tid; q < gc.npts; q += nth) {
-        int I = (int)(q % gc.m);
-        long t = q / gc.m;
-        int J = (int)(t % gc.n);
-        int K = (int)(t / gc.n);
+        int I, J, K;
+        decode_nat(gc, q, I, J, K);
         T acc = T(0);
         for (int cz = K - 1; cz <= K; cz++) {
             if (cz < 0 || cz > lz) continue;
@@ -148,10 +142,8 @@ template <class T>
 __device__ __forceinline__ void c_interp(const LevelGeom& gf, const LevelGeom& gc, T* xf, const T* xcv, int tid,
                                          int nth) {
     for (long q = tid; q < gf.npts; q += nth) {
-        int i = (int)(q % gf.m);
-        long t = q / gf.m;
-        int j = (int)(t % gf.n);
-        int k = (int)(t / gf.n);
+        int i, j, k;
+        decode_nat(gf, q, i, j, k);
         int Cx = i >> 1, Cy = j >> 1, Cz = k >> 1, dx = i & 1, dy = j & 1, dz = k & 1;
         long b = gc.xi(Cx, Cy, Cz);
         long sy = gc.mx, sz = gc.mx * gc.my;

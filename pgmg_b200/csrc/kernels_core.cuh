@@ -39,10 +39,8 @@ __device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ 
 template <class T>
 __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* __restrict__ r,
                                              const T* __restrict__ A, int col, long p) {
-    int i2 = (int)(p % g.M2);
-    long t = p / g.M2;
-    int j2 = (int)(t % g.N2);
-    int k2 = (int)(t / g.N2);
+    int i2, j2, k2;
+    decode_colour(g, p, i2, j2, k2);
     int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
     if (i >= g.m || j >= g.n || k >= g.o) return;
     uint64_t ps = policy_evict_first(), pk = policy_evict_last();
@@ -169,10 +167,8 @@ __global__ void __launch_bounds__(1024) k_gs_mc8_block(LevelGeom g, T* x, const 
                 for (int cc = 0; cc < 8; cc++) {
                     int col = pass ? 7 - cc : cc;
                     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-                        int i2 = (int)(p % g.M2);
-                        long t = p / g.M2;
-                        int j2 = (int)(t % g.N2);
-                        int k2 = (int)(t / g.N2);
+                        int i2, j2, k2;
+                        decode_colour(g, p, i2, j2, k2);
                         int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
                         if (i >= g.m || j >= g.n || k >= g.o) continue;
                         long xc = g.xi(i, j, k);
@@ -224,10 +220,8 @@ __device__ __forceinline__ void residual_at(const LevelGeom& g, const T* __restr
                                             double& s_res, double& s_rhs) {
     long nc = (long)g.M2 * g.N2 * g.O2;
     if (p >= nc) return;
-    int i2 = (int)(p % g.M2);
-    long t = p / g.M2;
-    int j2 = (int)(t % g.N2);
-    int k2 = (int)(t / g.N2);
+    int i2, j2, k2;
+    decode_colour(g, p, i2, j2, k2);
     int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
     if (i >= g.m || j >= g.n || k >= g.o) return;
     uint64_t ps = policy_evict_first(), pk = policy_evict_last();
@@ -312,10 +306,8 @@ template <class T>
 __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
                                             T* __restrict__ rc, T* __restrict__ xc, long q) {
     if (q >= gc.npts) return;
-    int I = (int)(q % gc.m);
-    long t = q / gc.m;
-    int J = (int)(t % gc.n);
-    int K = (int)(t / gc.n);
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
     int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
     T acc = T(0);
     for (int cz = K - 1; cz <= K; cz++) {
@@ -365,10 +357,8 @@ template <class T>
 __device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& gc, T* __restrict__ xf,
                                           const T* __restrict__ xcv, long q) {
     if (q >= gf.npts) return;
-    int i = (int)(q % gf.m);
-    long t = q / gf.m;
-    int j = (int)(t % gf.n);
-    int k = (int)(t / gf.n);
+    int i, j, k;
+    decode_nat(gf, q, i, j, k);
     int Cx = i >> 1, Cy = j >> 1, Cz = k >> 1, dx = i & 1, dy = j & 1, dz = k & 1;
     long b = gc.xi(Cx, Cy, Cz);
     long sy = gc.mx, sz = gc.mx * gc.my;
@@ -425,28 +415,32 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) k_nat_to_x(LevelGeom g, const double* __restrict__ src, T* __restrict__ x) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     x[g.xi(i, j, k)] = (T)src[q];
 }
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_x_to_nat(LevelGeom g, const T* __restrict__ x, double* __restrict__ dst) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     dst[q] = (double)x[g.xi(i, j, k)];
 }
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_nat_to_cm(LevelGeom g, const double* __restrict__ src, T* __restrict__ r) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     r[g.ri(i, j, k)] = (T)src[q];
 }
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_cm_to_nat(LevelGeom g, const T* __restrict__ r, double* __restrict__ dst) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     dst[q] = (double)r[g.ri(i, j, k)];
 }
 
@@ -487,7 +481,8 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) k_clear_x(LevelGeom g, T* __restrict__ x) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     x[g.xi(i, j, k)] = T(0);
 }
 
@@ -496,7 +491,8 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) k_setup_test(LevelGeom g, T* x, T* r, int ca, int xfield) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     T v;
     switch (ca) {
         case 0: v = i; break;
@@ -518,7 +514,8 @@ __global__ void __launch_bounds__(kBlock) k_apply(LevelGeom g, const T* __restri
                                                   double* __restrict__ out) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     double acc = 0.0;
     for (int s = 0; s < 27; s++) {
         int ii = i + s % 3 - 1, jj = j + (s / 3) % 3 - 1, kk = k + s / 9 - 1;
@@ -540,7 +537,8 @@ static __global__ void __launch_bounds__(kBlock) k_add_correction(LevelGeom g, d
                                                            const float* __restrict__ e32) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     long c = g.xi(i, j, k);
     x64[c] = x64[c] + (double)e32[c];
 }

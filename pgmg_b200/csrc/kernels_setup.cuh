@@ -43,7 +43,8 @@ static __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGe
                                                     int8_t* __restrict__ Sc) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= gc.npts) return;
-    int I = (int)(q % gc.m); long t = q / gc.m; int J = (int)(t % gc.n); int K = (int)(t / gc.n);
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
     int s[6] = {0, 1, 0, 1, 0, 1};
     AxisList X = axis_list(I, gf.m), Y = axis_list(J, gf.n), Z = axis_list(K, gf.o);
     for (int c = 0; c < Z.n; c++)
@@ -75,7 +76,8 @@ static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom
                                                   const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= gc.npts) return;
-    int I = (int)(q % gc.m); long t = q / gc.m; int J = (int)(t % gc.n); int K = (int)(t / gc.n);
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
     double acc[27];
 #pragma unroll
     for (int s = 0; s < 27; s++) acc[s] = 0.0;
@@ -340,7 +342,8 @@ static __global__ void __launch_bounds__(128) k_assemble_q1(LevelGeom g, const d
                                                      int8_t* __restrict__ S) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     long nx = g.m - 1, ny = g.n - 1;
     const double khat[4] = {1.0 / 3.0, 0.0, -1.0 / 12.0, -1.0 / 12.0};
     double c[27];
@@ -392,7 +395,8 @@ __device__ __forceinline__ uint64_t d_splitmix64(uint64_t z) {
 static __global__ void __launch_bounds__(256) k_rhs_uniform(LevelGeom g, uint64_t seed, double* __restrict__ r) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
-    int i = (int)(q % g.m); long t = q / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
     uint64_t key = (seed + 0x5851F42D4C957F2Dull) * 0x2545F4914F6CDD1Dull;
     bool interior = i > 0 && i < g.m - 1 && j > 0 && j < g.n - 1 && k > 0 && k < g.o - 1;
     double v = 0.0;

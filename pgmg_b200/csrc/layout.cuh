@@ -53,6 +53,24 @@ struct LevelGeom {
     }
 };
 
+// Index decoding with 32-bit unsigned division (index spaces stay below
+// 2^32 points for every supported size; 64-bit division costs several times
+// more instructions per thread).
+__host__ __device__ __forceinline__ void decode_colour(const LevelGeom& g, long p, int& i2, int& j2, int& k2) {
+    unsigned u = (unsigned)p, M2 = (unsigned)g.M2, N2 = (unsigned)g.N2;
+    unsigned t = u / M2;
+    i2 = (int)(u - t * M2);
+    k2 = (int)(t / N2);
+    j2 = (int)(t - (unsigned)k2 * N2);
+}
+__host__ __device__ __forceinline__ void decode_nat(const LevelGeom& g, long q, int& i, int& j, int& k) {
+    unsigned u = (unsigned)q, m = (unsigned)g.m, n = (unsigned)g.n;
+    unsigned t = u / m;
+    i = (int)(u - t * m);
+    k = (int)(t / n);
+    j = (int)(t - (unsigned)k * n);
+}
+
 inline LevelGeom make_geom(int m, int n, int o) {
     LevelGeom g;
     g.m = m; g.n = n; g.o = o;
