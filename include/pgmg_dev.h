@@ -234,6 +234,26 @@ pgmg_status pgmg_dev_fmg_cycle(pgmg_handle *h, int smoother);
  * (region.cc:1549-1558).  Either output may be NULL. */
 pgmg_status pgmg_dev_norms(pgmg_handle *h, int level, double *res2, double *rhs2);
 
+/* Allocation-free residual norms.  No counterpart in the reference: this is
+ * for callers that cannot allocate device memory -- code under a host
+ * framework that owns all of the card's memory through its own pool, or a
+ * latency-critical loop where a cudaMalloc/cudaFree would stall or
+ * synchronise the device.  Given caller-owned device arrays of an m x n x o
+ * grid (natural order: coef27 with 27 slots per point, slot
+ * (di+1)+3(dj+1)+9(dk+1); x and r with one value per point) it writes
+ * out[0] = sum (r - A x)^2 and out[1] = sum r^2 (out: 2 device doubles),
+ * asynchronously on `stream` (NULL = the default stream); read out after the
+ * stream has finished.  It allocates nothing: its partial sums live in a
+ * fixed 1 MiB array inside this library that every GPU loading it holds until
+ * the process exits, so m*n*o is limited to 16,777,216 points (PGMG_ERR_ARG
+ * beyond that, and for host pointers).  The first call on a device looks up
+ * that array's device address; make that first call before any stream
+ * capture.  All calls on a device share the array (each overwrites every
+ * partial sum it reads, so nothing has to be cleared): calls that overlap on
+ * the GPU race and must be serialised by the caller. */
+pgmg_status pgmg_residual_norms_noalloc(int m, int n, int o, const double *coef27, const double *x,
+                                        const double *r, double *out, void *stream);
+
 /* ---- solves ----------------------------------------------------------- */
 
 /* multigrid::solve_v_cycles (multigrid.hh:182-219) with its mg_guide:

@@ -104,6 +104,7 @@ SIGNATURES = [
     ("pgmg_dev_create_in", C.c_int, [C.POINTER(Dims), _VP, C.c_size_t, C.POINTER(C.c_void_p)]),
     ("pgmg_dev_assemble_q1", C.c_int, [_VP, _VP, C.c_int, C.c_double]),
     ("pgmg_dev_rhs_uniform", C.c_int, [_VP, C.c_uint64]),
+    ("pgmg_residual_norms_noalloc", C.c_int, [C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP]),
     ("pgmg_problem_gauss", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_double, _dp]),
     ("pgmg_problem_kappa", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_double, _dp]),
     ("pgmg_problem_q1", C.c_int, [C.c_int, C.c_int, C.c_int, _VP, _dp, _VP]),
@@ -170,6 +171,17 @@ def problem_rhs(m: int, n: int, o: int, seed: int) -> np.ndarray:
     if st:
         raise PgmgError(st, "pgmg_problem_rhs")
     return out
+
+
+def residual_norms_noalloc(m: int, n: int, o: int, coef27_ptr: int, x_ptr: int, r_ptr: int, out_ptr: int,
+                           stream_ptr: int | None = None) -> None:
+    """sum (r - A x)^2 and sum r^2 into out (2 device doubles) from
+    caller-owned device arrays, without allocating device memory (for callers
+    whose framework owns all device memory, or whose loops must not stall in
+    an allocation); at most 16,777,216 points; see pgmg_dev.h."""
+    st = lib().pgmg_residual_norms_noalloc(m, n, o, coef27_ptr, x_ptr, r_ptr, out_ptr, stream_ptr)
+    if st:
+        raise PgmgError(st, "pgmg_residual_norms_noalloc")
 
 
 def plan_bytes(m, n, o, precision=FP64) -> int:

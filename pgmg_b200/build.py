@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "-I" + os.path.join(ROOT, "include")]
 
-SOURCES = ["capi.cu", "batch.cu", "problems.cpp"]
+SOURCES = ["capi.cu", "batch.cu", "noalloc.cu", "problems.cpp"]
 
 
 def _newer(src_list, target):
