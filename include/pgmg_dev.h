@@ -128,8 +128,7 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
 /* Execution options (tuning; results do not depend on them unless noted).
  *   PGMG_OPT_GRAPHS         1 = replay each V-cycle as a captured CUDA graph (default)
  *   PGMG_OPT_CLUSTER_FIRST  first level run by the one-cluster coarse cycle
- *                           (default: the first level of <= 50000 points,
- *                           <= 10000 for PGMG_MIXED handles;
+ *                           (default: the first level of <= 50000 points;
  *                           = number of levels disables it)
  *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 16, 8, or 0 (off)
  *   PGMG_OPT_SLAB_BUDGET    bytes of solution vector per z-slab of the 8-colour
@@ -139,7 +138,11 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *   PGMG_OPT_V_DOWN, PGMG_OPT_V_UP, PGMG_OPT_V_BOTTOM
  *                           the reference's public sweep counts (multigrid.hh:
  *                           122-128; defaults 2, 2, 20): level l gets v_down+l
- *                           pre- and v_up+l-1 post-sweeps (multigrid.cc:92,102). */
+ *                           pre- and v_up+l-1 post-sweeps (multigrid.cc:92,102).
+ *   PGMG_OPT_PDL            1 = launch the V-cycle's kernels as programmatic
+ *                           dependent launches, so that each is scheduled while
+ *                           the one before it drains (default); 0 = plain
+ *                           launches.  No counterpart in the reference. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -147,7 +150,8 @@ enum {
     PGMG_OPT_SLAB_BUDGET = 4,
     PGMG_OPT_V_DOWN = 5,
     PGMG_OPT_V_UP = 6,
-    PGMG_OPT_V_BOTTOM = 7
+    PGMG_OPT_V_BOTTOM = 7,
+    PGMG_OPT_PDL = 8
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
@@ -264,9 +268,13 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle *h, double p_scale, int *result,
                                     double *res2, int *cycles);
 /* Relative-residual solve: V-cycles from the current x until
  * sqrt(sum r^2 / sum b^2) < tol or max_cycles.  PGMG_MIXED handles run FP64
- * iterative refinement around FP32 V-cycles.  check_every: residual check
- * period in cycles (>= 1), or 0 for an adaptive schedule that predicts the
- * remaining cycles from the observed reduction factor.  Outputs may be NULL. */
+ * iterative refinement around FP32 V-cycles: each step computes the FP64
+ * residual (and checks it), solves for the correction with FP32 V-cycles from
+ * zero, and adds it in FP64.  check_every: residual check period in cycles
+ * (>= 1; in mixed precision the FP32 V-cycles per refinement step), or 0 for
+ * an adaptive schedule that predicts the remaining cycles from the observed
+ * reduction factor (mixed precision: up to 16 cycles per step, and no more
+ * than a 1e-5 predicted reduction).  Outputs may be NULL. */
 pgmg_status pgmg_dev_solve_relres(pgmg_handle *h, double tol, int max_cycles, int check_every,
                                   int *cycles, double *relres);
 
@@ -302,6 +310,8 @@ pgmg_status pgmg_batch_begin(pgmg_batch *b, int slot);
 pgmg_status pgmg_batch_step(pgmg_batch *b, double tol, int max_cycles, int *n_active);
 pgmg_status pgmg_batch_poll(pgmg_batch *b, int *active, int *cycles, double *relres);
 pgmg_status pgmg_batch_set_graphs(pgmg_batch *b, int on);
+/* PGMG_OPT_GRAPHS and PGMG_OPT_PDL for the batch's step launches. */
+pgmg_status pgmg_batch_set_option(pgmg_batch *b, int key, long long value);
 
 /* ---- host problem generators (no GPU needed) ---------------------------- */
 

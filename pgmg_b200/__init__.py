@@ -27,6 +27,7 @@ COARSE_LU, COARSE_GS, COARSE_LU_EXACT = 0, 1, 2
 FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
 OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE, OPT_SLAB_BUDGET = 1, 2, 3, 4
 OPT_V_DOWN, OPT_V_UP, OPT_V_BOTTOM = 5, 6, 7
+OPT_PDL = 8
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -101,6 +102,7 @@ SIGNATURES = [
     ("pgmg_batch_step", C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int)]),
     ("pgmg_batch_poll", C.c_int, [_VP, _VP, _VP, _VP]),
     ("pgmg_batch_set_graphs", C.c_int, [_VP, C.c_int]),
+    ("pgmg_batch_set_option", C.c_int, [_VP, C.c_int, C.c_longlong]),
     ("pgmg_dev_create_in", C.c_int, [C.POINTER(Dims), _VP, C.c_size_t, C.POINTER(C.c_void_p)]),
     ("pgmg_dev_assemble_q1", C.c_int, [_VP, _VP, C.c_int, C.c_double]),
     ("pgmg_dev_rhs_uniform", C.c_int, [_VP, C.c_uint64]),
@@ -486,6 +488,10 @@ class Batch:
 
     def set_graphs(self, on: bool):
         self._ck(lib().pgmg_batch_set_graphs(self._b, int(on)), "batch_set_graphs")
+
+    def set_option(self, key: int, value: int):
+        """OPT_GRAPHS or OPT_PDL for the batch's step launches."""
+        self._ck(lib().pgmg_batch_set_option(self._b, int(key), int(value)), "batch_set_option")
 
     @property
     def launches(self) -> int:

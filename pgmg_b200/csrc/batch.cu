@@ -69,6 +69,7 @@ __device__ __forceinline__ int map_entry(const BMap* __restrict__ M, int b) {
 template <class T>
 __global__ void __launch_bounds__(kBlock) kb_gs_colour(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                        const int* __restrict__ active, int lev, int col) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -84,6 +85,7 @@ __global__ void __launch_bounds__(kBlock) kb_gs_colour(const BSlot<T>* __restric
 template <class T>
 __global__ void __launch_bounds__(kBlock) kb_residual(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                       const int* __restrict__ active, int lev) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -99,6 +101,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual(const BSlot<T>* __restrict
 template <class T>
 __global__ void __launch_bounds__(kBlock) kb_restrict(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                       const int* __restrict__ active, int lc) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -110,6 +113,7 @@ __global__ void __launch_bounds__(kBlock) kb_restrict(const BSlot<T>* __restrict
 template <class T>
 __global__ void __launch_bounds__(kBlock) kb_interp(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                     const int* __restrict__ active, int lc) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -124,6 +128,7 @@ __global__ void __launch_bounds__(kBlock) kb_interp(const BSlot<T>* __restrict__
 template <class T, class TO>
 __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                    const int* __restrict__ active, const int* __restrict__ first) {
+    pdl_enter();
     __shared__ double sh[64];
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
@@ -163,6 +168,7 @@ __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S
                                                   int* __restrict__ active, int* __restrict__ first,
                                                   int* __restrict__ cycles, double* __restrict__ relres,
                                                   double tol, int max_cycles) {
+    pdl_enter();
     __shared__ double sh[64];
     int s = M->slot[blockIdx.x];
     if (!active[s]) return;
@@ -186,6 +192,7 @@ __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S
 
 __global__ void __launch_bounds__(kBlock) kb_clear32(const BSlot<float>* __restrict__ S, const BMap* __restrict__ M,
                                                      const int* __restrict__ active) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -199,6 +206,7 @@ __global__ void __launch_bounds__(kBlock) kb_clear32(const BSlot<float>* __restr
 
 __global__ void __launch_bounds__(kBlock) kb_add32(const BSlot<float>* __restrict__ S, const BMap* __restrict__ M,
                                                    const int* __restrict__ active) {
+    pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
     if (!active[s]) return;
@@ -279,6 +287,7 @@ struct pgmg_batch {
     int stable_steps = 0;  // steps run since the last shape change (capture from the second)
     long long graph_nodes = 0;  // kernels in the captured step
     bool use_graphs = true;
+    bool pdl = true;  // step kernels as programmatic dependent launches
     double cap_tol = -1;  // tol and cycle cap the step graphs were captured with
     int cap_max = -1;
     long long launches = 0;
@@ -426,6 +435,12 @@ pgmg_status build_shape(pgmg_batch* b) {
     return PGMG_OK;
 }
 
+// A step kernel (one that starts with pdl_enter()).
+#define BLAUNCH(grid, block, ...)                                      \
+    do {                                                               \
+        b->launches++;                                                 \
+        BCK(launch_k(b->stream, b->pdl, grid, block, __VA_ARGS__));    \
+    } while (0)
 #define BKL()                           \
     do {                                \
         b->launches++;                  \
@@ -437,40 +452,36 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
     const BSlot<T>* S = static_cast<const BSlot<T>*>(b->slot_table);
     auto M = [&](int m) { return b->maps + m; };
     using TO = T;
-    kb_check<T, TO><<<map_blocks(b, b->map_chk), kBlock, 0, b->stream>>>(S, M(b->map_chk), b->active, b->first);
-    BKL();
-    kb_reduce<T><<<(int)b->members.size(), 1024, 0, b->stream>>>(S, M(b->map_red), b->active, b->first, b->cycles,
+    BLAUNCH(map_blocks(b, b->map_chk), kBlock, kb_check<T, TO>, S, M(b->map_chk), b->active, b->first);
+    BLAUNCH((int)b->members.size(), 1024, kb_reduce<T>, S, M(b->map_red), b->active, b->first, b->cycles,
                                                                   b->relres, tol, max_cycles);
-    BKL();
     if (std::is_same<T, float>::value) {
-        kb_clear32<<<map_blocks(b, b->map_pt0), kBlock, 0, b->stream>>>(
+        BLAUNCH(map_blocks(b, b->map_pt0), kBlock, kb_clear32, 
             reinterpret_cast<const BSlot<float>*>(S), M(b->map_pt0), b->active);
-        BKL();
     }
     for (int l = 0; l < b->maxtop; l++) {
         if (b->map_gs[l] < 0) continue;
         for (int sw = 0; sw < b->v_down + l; sw++)
             for (int c = 0; c < 8; c++) {
-                kb_gs_colour<T><<<map_blocks(b, b->map_gs[l]), kBlock, 0, b->stream>>>(S, M(b->map_gs[l]), b->active, l, c);
-                BKL();
+                BLAUNCH(map_blocks(b, b->map_gs[l]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l]), b->active, l, c);
             }
-        kb_residual<T><<<map_blocks(b, b->map_res[l]), kBlock, 0, b->stream>>>(S, M(b->map_res[l]), b->active, l);
-        BKL();
-        kb_restrict<T><<<map_blocks(b, b->map_rst[l + 1]), kBlock, 0, b->stream>>>(S, M(b->map_rst[l + 1]), b->active, l + 1);
-        BKL();
+        BLAUNCH(map_blocks(b, b->map_res[l]), kBlock, kb_residual<T>, S, M(b->map_res[l]), b->active, l);
+        BLAUNCH(map_blocks(b, b->map_rst[l + 1]), kBlock, kb_restrict<T>, S, M(b->map_rst[l + 1]), b->active, l + 1);
     }
     {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(b->members.size() * b->csize), 1, 1);
         cfg.blockDim = dim3(kClusterThreads, 1, 1);
         cfg.stream = b->stream;
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = b->csize;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = b->pdl ? 2 : 1;
         const CoarsePlan<T>* plans = static_cast<const CoarsePlan<T>*>(b->plan_table);
         const int* cs = b->cluster_slots;
         const int* act = b->active;
@@ -479,18 +490,15 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
     }
     for (int l = b->maxtop; l > 0; l--) {
         if (b->map_int[l] < 0) continue;
-        kb_interp<T><<<map_blocks(b, b->map_int[l]), kBlock, 0, b->stream>>>(S, M(b->map_int[l]), b->active, l);
-        BKL();
+        BLAUNCH(map_blocks(b, b->map_int[l]), kBlock, kb_interp<T>, S, M(b->map_int[l]), b->active, l);
         for (int sw = 0; sw < b->v_up + l - 1; sw++)
             for (int c = 0; c < 8; c++) {
-                kb_gs_colour<T><<<map_blocks(b, b->map_gs[l - 1]), kBlock, 0, b->stream>>>(S, M(b->map_gs[l - 1]), b->active, l - 1, c);
-                BKL();
+                BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, c);
             }
     }
     if (std::is_same<T, float>::value) {
-        kb_add32<<<map_blocks(b, b->map_pt0), kBlock, 0, b->stream>>>(reinterpret_cast<const BSlot<float>*>(S),
+        BLAUNCH(map_blocks(b, b->map_pt0), kBlock, kb_add32, reinterpret_cast<const BSlot<float>*>(S),
                                                                         M(b->map_pt0), b->active);
-        BKL();
     }
     return PGMG_OK;
 }
@@ -706,6 +714,17 @@ pgmg_status pgmg_batch_set_graphs(pgmg_batch* b, int on) {
     if (!b) return PGMG_ERR_ARG;
     drop_step_graphs(b);
     b->use_graphs = on != 0;
+    return PGMG_OK;
+}
+
+pgmg_status pgmg_batch_set_option(pgmg_batch* b, int key, long long value) {
+    if (!b) return PGMG_ERR_ARG;
+    switch (key) {
+        case PGMG_OPT_GRAPHS: b->use_graphs = value != 0; break;
+        case PGMG_OPT_PDL: b->pdl = value != 0; break;
+        default: return bfail(b, PGMG_ERR_ARG, "unknown batch option %d", key);
+    }
+    drop_step_graphs(b);
     return PGMG_OK;
 }
 

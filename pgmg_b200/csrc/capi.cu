@@ -35,6 +35,12 @@ pgmg_status fail(pgmg_handle* h, pgmg_status st, const char* fmt, ...) {
         h->launches++;    \
         CK(cudaGetLastError()); \
     } while (0)
+// A V-cycle or solve-loop kernel (one that starts with pdl_enter()).
+#define LAUNCH(grid, block, ...)                                              \
+    do {                                                                      \
+        h->launches++;                                                        \
+        CK(launch_k(h->stream, h->pdl, grid, block, __VA_ARGS__));            \
+    } while (0)
 #define TRY(expr)                          \
     do {                                   \
         pgmg_status s_ = (expr);           \
@@ -121,8 +127,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
     const LevelGeom& g = L.g;
     if (smoother == PGMG_SMOOTH_LEX) {
         if (g.npts <= kLexBlockMax) {
-            k_gs_lex_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode);
-            CKL();
+            LAUNCH(1, 1024, k_gs_lex_block<T>, g, v.x, v.r, v.A, sweeps, mode);
             return PGMG_OK;
         }
         int np = num_planes(g);
@@ -133,14 +138,12 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                     Plane P = plane_range(g, t);
                     long nw = (long)(P.kmax - P.kmin + 1) * P.jw;
                     if (nw <= 0) continue;
-                    k_gs_plane<T><<<nblk(nw), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, t, P);
-                    CKL();
+                    LAUNCH(nblk(nw), kBlock, k_gs_plane<T>, g, v.x, v.r, v.A, t, P);
                 }
         return PGMG_OK;
     }
     if (g.npts <= kMc8BlockMax) {
-        k_gs_mc8_block<T><<<1, 1024, 0, h->stream>>>(g, v.x, v.r, v.A, sweeps, mode, h->slab_budget);
-        CKL();
+        LAUNCH(1, 1024, k_gs_mc8_block<T>, g, v.x, v.r, v.A, sweeps, mode, h->slab_budget);
         return PGMG_OK;
     }
     int S = slab_count(g, (int)sizeof(T), h->slab_budget);
@@ -152,8 +155,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 long np = (long)(k2hi - k2lo) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
                     int col = pass ? 7 - cc : cc;
-                    k_gs_colour<T, true><<<nblk(np), kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, col, k2lo, k2hi);
-                    CKL();
+                    LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
                 }
             }
     return PGMG_OK;
@@ -165,8 +167,7 @@ pgmg_status residual_level(pgmg_handle* h, int l, T* out, double* partials) {
     View<T> v = view<T>(L);
     const LevelGeom& g = L.g;
     dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
-    k_residual<T, T, true><<<grid, kBlock, 0, h->stream>>>(g, v.x, v.r, v.A, out, partials);
-    CKL();
+    LAUNCH(grid, kBlock, k_residual<T, T, true>, g, v.x, v.r, v.A, out, partials);
     return PGMG_OK;
 }
 
@@ -176,8 +177,7 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     Level& Cl = h->L[l];
     View<T> vf = view<T>(F), vc = view<T>(Cl);
     TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
-    k_restrict<T><<<nblk(Cl.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, vf.res, vc.r, vc.x);
-    CKL();
+    LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
     return PGMG_OK;
 }
 
@@ -185,8 +185,7 @@ template <class T>
 pgmg_status interp_level(pgmg_handle* h, int l) {
     Level& F = h->L[l - 1];
     Level& Cl = h->L[l];
-    k_interp<T><<<nblk(F.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
-    CKL();
+    LAUNCH(nblk(F.g.npts), kBlock, k_interp<T>, F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
     return PGMG_OK;
 }
 
@@ -197,12 +196,11 @@ pgmg_status coarse_solve_t(pgmg_handle* h, int smoother) {
     View<T> v = view<T>(L);
     if (h->lu_ok) {
         if (h->dims.coarse == PGMG_COARSE_LU_EXACT) {
-            k_lu_solve_exact<T><<<1, 1024, 0, h->stream>>>(L.g, h->M, h->piv, v.r, v.x, h->lubuf);
+            LAUNCH(1, 1024, k_lu_solve_exact<T>, L.g, h->M, h->piv, v.r, v.x, h->lubuf);
         } else {
             long thr = L.g.npts * 32;
-            k_lu_apply<T><<<nblk(thr), kBlock, 0, h->stream>>>(L.g, h->Minv, v.r, v.x);
+            LAUNCH(nblk(thr), kBlock, k_lu_apply<T>, L.g, h->Minv, v.r, v.x);
         }
-        CKL();
         return PGMG_OK;
     }
     // region::solve_exact fallback: pgmg_gs_exact plain (mode 0) sweeps of
@@ -253,13 +251,15 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     cfg.gridDim = dim3(h->cluster_size, 1, 1);
     cfg.blockDim = dim3(kClusterThreads, 1, 1);
     cfg.stream = h->stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = h->cluster_size;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = h->pdl ? 2 : 1;
     const int* no_map = nullptr;
     const int* no_flags = nullptr;
     CK(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, plan_of<T>(h), no_map, no_flags, mode));
@@ -386,8 +386,7 @@ pgmg_status norms64(pgmg_handle* h, int l, double* res2, double* rhs2) {
     Level& L = h->L[l];
     TRY(residual_level<double>(h, l, nullptr, h->partials));
     long nb = nblk((long)L.g.M2 * L.g.N2 * L.g.O2) * 8;
-    k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
-    CKL();
+    LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
     CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (res2) *res2 = h->norm_host[0];
@@ -402,22 +401,18 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
     Level& L0 = h->L[0];
     const LevelGeom& g = L0.g;
     dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
-    k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
-    CKL();
+    LAUNCH(grid, kBlock, k_residual<double, float, true>, g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
-    k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
-    CKL();
+    LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
     if (res2 || rhs2) {
         CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         if (res2) *res2 = h->norm_host[0];
         if (rhs2) *rhs2 = h->norm_host[1];
     }
-    k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
-    CKL();
+    LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
     TRY(run_vcycle<float>(h, mode, smoother));
-    k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
-    CKL();
+    LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
     return PGMG_OK;
 }
 
@@ -568,9 +563,8 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
         }
     }
     h->coarse_first = h->nl - 1;
-    long cmax = dims->precision == PGMG_MIXED ? kClusterMax32 : kClusterMax;
     for (int l = 0; l < h->nl; l++)
-        if (h->L[l].g.npts <= cmax) { h->coarse_first = l; break; }
+        if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
     if (cudaMemsetAsync(h->arena.base, 0, bytes, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         pgmg_dev_destroy(h);
@@ -636,6 +630,9 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_SLAB_BUDGET:
             h->slab_budget = value;
             break;
+        case PGMG_OPT_PDL:
+            h->pdl = value != 0;
+            break;
         case PGMG_OPT_V_DOWN:
         case PGMG_OPT_V_UP:
         case PGMG_OPT_V_BOTTOM:
@@ -660,6 +657,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_V_DOWN: *value = h->v_down; return PGMG_OK;
         case PGMG_OPT_V_UP: *value = h->v_up; return PGMG_OK;
         case PGMG_OPT_V_BOTTOM: *value = h->v_bottom; return PGMG_OK;
+        case PGMG_OPT_PDL: *value = h->pdl; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -882,8 +880,7 @@ pgmg_status pgmg_dev_apply(pgmg_handle* h, int level, const double* in, double* 
 pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
     if (level == 0) h->x0_zero = true;
-    k_clear_x<double><<<nblk(h->L[level].g.npts), kBlock, 0, h->stream>>>(h->L[level].g, h->L[level].x64);
-    CKL();
+    LAUNCH(nblk(h->L[level].g.npts), kBlock, k_clear_x<double>, h->L[level].g, h->L[level].x64);
     return PGMG_OK;
 }
 
@@ -1002,15 +999,18 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result,
 }
 
 // Residual-check schedule of the relative-residual solve.  check_every >= 1:
-// every that many cycles.  check_every == 0: adaptive -- after two checks the
-// per-cycle reduction factor is estimated from the last two residuals and
-// the solve runs one cycle fewer than predicted before checking again, so a
-// converged solve rarely pays for more than one check past the prediction.
+// every that many cycles.  check_every == 0: adaptive -- the per-cycle
+// reduction factor is estimated from the last two checks (or remembered from
+// the handle's previous solve) and the solve runs the cycles predicted to
+// reach tol before checking again, stopping one short when that one might
+// already be enough.
+constexpr double kSlack = 3.0;
+
 struct CheckPlan {
     int every;
     double rho0 = 0;  // reduction factor remembered from an earlier solve
-    int last_n = -1, prev_n = -1;
-    double last_r = 0, prev_r = 0;
+    int last_n = -1, prev_n = -1, first_n = -1;
+    double last_r = 0, prev_r = 0, first_r = 0;
     double rho() const {
         if (prev_n >= 0 && last_r > 0 && prev_r > 0) return pow(last_r / prev_r, 1.0 / (last_n - prev_n));
         return rho0;
@@ -1022,13 +1022,23 @@ struct CheckPlan {
         double need = log(tol / last_r) / log(q);
         int n = (int)ceil(need);
         if (n < 1) n = 1;
-        // Run the predicted count only when it lands well below tol;
-        // otherwise stop one cycle short and check again.
-        bool margin = last_r * pow(q, n) < 0.3 * tol;
-        return nc + (margin || n == 1 ? n : n - 1);
+        // The reduction factor is an estimate: when the cycle before the
+        // predicted one might already reach tol (its predicted residual is
+        // within kSlack of tol), check after it -- a check costs a fraction
+        // of a cycle, a needless cycle costs a whole one.
+        if (n > 1 && last_r * pow(q, n - 1) < kSlack * tol) n--;
+        return nc + n;
     }
-    void record(int nc, double r) { prev_n = last_n; prev_r = last_r; last_n = nc; last_r = r; }
+    void record(int nc, double r) {
+        if (first_n < 0) { first_n = nc; first_r = r; }
+        prev_n = last_n; prev_r = last_r; last_n = nc; last_r = r;
+    }
 };
+
+// Mixed precision: the largest reduction asked of the FP32 V-cycles of one
+// refinement step, and the most cycles one step runs.
+constexpr double kInnerReduction = 1e-5;
+constexpr int kInnerMax = 16;
 
 pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
                                   double* relres) {
@@ -1047,27 +1057,25 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
     bool mixed = h->dims.precision == PGMG_MIXED;
     plan.rho0 = h->last_rho;
     for (;;) {
-        bool check = nc >= next_check || nc >= max_cycles;
+        // Mixed precision computes the FP64 residual at every refinement step
+        // (it is the next correction's source), so it checks every step too.
+        bool check = mixed || nc >= next_check || nc >= max_cycles;
         bool zero = nc == 0 && h->x0_zero;  // residual = source: no stencil pass needed
         if (zero) {
             if (mixed || check) {
-                k_source<double, float><<<grid, kBlock, 0, h->stream>>>(g, L0.r64, mixed ? L0.r32 : nullptr, h->partials);
-                CKL();
+                LAUNCH(grid, kBlock, k_source<double, float>, g, L0.r64, mixed ? L0.r32 : nullptr, h->partials);
             }
         } else if (mixed) {
             // FP64 residual of the current x, stored FP32 as the correction's
             // source (and reduced to the norms when checking).
-            k_residual<double, float, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, L0.r32,
+            LAUNCH(grid, kBlock, k_residual<double, float, true>, g, L0.x64, L0.r64, L0.A64, L0.r32,
                                                                               check ? h->partials : nullptr);
-            CKL();
         } else if (check) {
-            k_residual<double, double, true><<<grid, kBlock, 0, h->stream>>>(g, L0.x64, L0.r64, L0.A64, nullptr,
+            LAUNCH(grid, kBlock, k_residual<double, double, true>, g, L0.x64, L0.r64, L0.A64, nullptr,
                                                                                h->partials);
-            CKL();
         }
         if (check) {
-            k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
-            CKL();
+            LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
             CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
             res2 = h->norm_host[0];
@@ -1080,22 +1088,35 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
         }
         h->x0_zero = false;
         if (mixed) {
-            k_clear_x<float><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x32);
-            CKL();
-            TRY(run_vcycle<float>(h, 0, smoother));
-            k_add_correction<<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, L0.x32);
-            CKL();
+            // One refinement step: A32 e = r32 solved by `inner` FP32
+            // V-cycles from e = 0, then x64 += e.  The count is the number of
+            // cycles the check schedule expects to run before its next check,
+            // capped so that one step asks the FP32 iteration for no more than
+            // a 1e-5 reduction (beyond that FP32 rounding, not the cycle count,
+            // limits what the correction can gain).
+            int inner = next_check - nc;
+            double q = plan.rho();
+            int cap = q > 0 && q < 0.9 ? (int)floor(log(kInnerReduction) / log(q)) : 1;
+            cap = cap < 1 ? 1 : cap > kInnerMax ? kInnerMax : cap;
+            if (plan.every == 0 && inner > cap) inner = cap;
+            if (inner > max_cycles - nc) inner = max_cycles - nc;
+            if (inner < 1) inner = 1;
+            LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
+            for (int i = 0; i < inner; i++) TRY(run_vcycle<float>(h, 0, smoother));
+            LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+            nc += inner;
+            continue;
         } else {
             TRY(run_vcycle<double>(h, 0, smoother));
         }
         nc++;
     }
-    if (plan.prev_n >= 0 && plan.last_n > plan.prev_n) {
-        double q = plan.rho();
-        if (q > 0 && q < 0.9) h->last_rho = q;
-    }
-    if (nc > 0 && rr < tol && plan.last_n >= 0 && nc > plan.last_n && plan.last_r > 0) {
-        double q = pow(rr / plan.last_r, 1.0 / (nc - plan.last_n));
+    // Remember the mean reduction per cycle over the whole solve: the next
+    // solve starts from its own first residual, and multigrid usually
+    // reduces faster in the first cycles than later, so the last interval's
+    // factor alone would overestimate the cycles a fresh solve needs.
+    if (nc > plan.first_n && plan.first_n >= 0 && plan.first_r > 0 && rr > 0) {
+        double q = pow(rr / plan.first_r, 1.0 / (nc - plan.first_n));
         if (q > 0 && q < 0.9) h->last_rho = q;
     }
     if (cycles) *cycles = nc;

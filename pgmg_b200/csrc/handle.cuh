@@ -2,6 +2,8 @@
 // by the single-problem entry points (capi.cu) and the batched solver
 // (batch.cu).
 #pragma once
+#include <utility>
+
 #include "../../include/pgmg_dev.h"
 #include "kernels_coarse.cuh"
 #include "kernels_core.cuh"
@@ -14,8 +16,7 @@ constexpr int kGsExact = 24;        // pgmg_gs_exact, common.hh:62
 constexpr int kMaxExact = 2048;     // pgmg_max_exact, common.hh:65
 constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicographically in one block
 constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
-constexpr long kClusterMax = 50000;   // FP64 V-cycle: levels up to this size run in the one-cluster coarse cycle
-constexpr long kClusterMax32 = 10000; // FP32 V-cycle (mixed handles): the same, measured lower break-even
+constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
 constexpr int kClusterThreads = 512;
 
 struct Level {
@@ -42,6 +43,24 @@ struct Arena {
         return p;
     }
 };
+
+// Launches k(args...) on `stream`; with `pdl` set, as a programmatic
+// dependent launch (k must start with pdl_enter(): it may be scheduled while
+// the previous kernel of the stream drains, and waits there for it).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(cudaStream_t stream, bool pdl, dim3 grid, dim3 block, void (*k)(KArgs...), Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
 
 }  // namespace pgmg
 
@@ -78,6 +97,7 @@ struct pgmg_handle {
     cudaGraphExec_t vgraph[2][2][2] = {};
     long long vgraph_nodes[2][2][2] = {};
     bool use_graphs = true;
+    bool pdl = true;  // V-cycle and solve-loop kernels as programmatic dependent launches
     // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
     // first level it handles.
     int cluster_size = 0;

@@ -37,10 +37,19 @@ struct CoarsePlan {
     const double* Minv;
 };
 
-__device__ __forceinline__ void cluster_sync() { cooperative_groups::this_cluster().sync(); }
+// Cluster barrier in its two halves: arrive (release: this thread's earlier
+// writes become visible to the cluster) and wait (acquire).  Loads of data
+// that no phase writes may be issued between the two, so that their latency
+// overlaps the barrier.
+__device__ __forceinline__ void cl_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cl_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_sync() {
+    cl_arrive();
+    cl_wait();
+}
 
 template <class T>
-__device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, const T* A, int col, long p0, long p1,
+__device__ __forceinline__ void c_colour(const LevelGeom g, T* x, const T* r, const T* A, int col, long p0, long p1,
                                          int tid, int nth) {
     for (long p = p0 + tid; p < p1; p += nth) {
         int i2, j2, k2;
@@ -60,10 +69,69 @@ __device__ __forceinline__ void c_colour(const LevelGeom& g, T* x, const T* r, c
     }
 }
 
+// Sweeps of a level whose colours have at most one point per thread (the
+// usual case: levels of <= 8 x 512 x cluster-size points), in one slab.
+// Thread tid owns colour point tid of every colour -- the same (i2,j2,k2),
+// decoded once -- and keeps the coefficients and source of its next colour
+// in registers, fetched between the halves of the barrier before that
+// colour's pass; only the neighbours' x values, which the previous pass may
+// have written, are loaded after it.  Same arithmetic as c_colour.
 template <class T>
-__device__ __forceinline__ void c_sweeps(const LevelGeom& g, T* x, const T* r, const T* A, int sweeps, int mode,
+__device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T* r, const T* A, int sweeps,
+                                               int mode, int tid) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    bool have = tid < nc;
+    int i0 = 0, j0 = 0, k0 = 0;
+    if (have) {
+        int i2, j2, k2;
+        decode_colour(g, tid, i2, j2, k2);
+        i0 = 2 * i2; j0 = 2 * j2; k0 = 2 * k2;
+    }
+    const long xc0 = g.xi(i0, j0, k0), sy = g.mx, sz = g.mx * g.my;
+    const int per = mode ? 16 : 8, total = sweeps * per;
+    T a[27];
+    T rv = T(0);
+    auto colour_at = [&](int st) {
+        int cc = st % per;
+        return cc < 8 ? cc : 15 - cc;
+    };
+    auto valid = [&](int col) {
+        return have && i0 + (col & 1) < g.m && j0 + ((col >> 1) & 1) < g.n && k0 + (col >> 2) < g.o;
+    };
+    auto fetch = [&](int col) {
+        if (!valid(col)) return;
+        const T* Ap = A + (long)col * 27 * g.Nc + tid;
+#pragma unroll
+        for (int q = 0; q < 27; q++) a[q] = __ldg(Ap + q * g.Nc);
+        rv = __ldcg(r + (long)col * g.Nc + tid);
+    };
+    if (total > 0) fetch(colour_at(0));
+    for (int st = 0; st < total; st++) {
+        int col = colour_at(st);
+        if (valid(col)) {
+            long xc = xc0 + (col & 1) + ((col >> 1) & 1) * sy + (col >> 2) * sz;
+            T acc = T(0);
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                if (q == 13) continue;
+                acc = madd<true, T>(acc, a[q], __ldcg(x + xc + slot_off(g, q)));
+            }
+            x[xc] = mul_rn<T>(sub_rn<T>(rv, acc), T(1) / a[13]);
+        }
+        cl_arrive();
+        if (st + 1 < total) fetch(colour_at(st + 1));
+        cl_wait();
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, const T* A, int sweeps, int mode,
                                          long long budget, int tid, int nth) {
     int S = slab_count(g, (int)sizeof(T), budget);
+    if (S == 1 && (long)g.M2 * g.N2 * g.O2 <= nth) {
+        c_sweeps_owned<T>(g, x, r, A, sweeps, mode, tid);
+        return;
+    }
     for (int s = 0; s < sweeps; s++)
         for (int pass = 0; pass < (mode ? 2 : 1); pass++)
             for (int ss = 0; ss < S; ss++) {
@@ -77,7 +145,7 @@ __device__ __forceinline__ void c_sweeps(const LevelGeom& g, T* x, const T* r, c
 }
 
 template <class T>
-__device__ __forceinline__ void c_residual(const LevelGeom& g, const T* x, const T* r, const T* A, T* res, int tid,
+__device__ __forceinline__ void c_residual(const LevelGeom g, const T* x, const T* r, const T* A, T* res, int tid,
                                            int nth) {
     long nc = (long)g.M2 * g.N2 * g.O2;
     for (long pp = tid; pp < 8 * nc; pp += nth) {
@@ -98,7 +166,7 @@ __device__ __forceinline__ void c_residual(const LevelGeom& g, const T* x, const
 
 // Same accumulation order as k_restrict (reference restriction order).
 template <class T>
-__device__ __forceinline__ void c_restrict(const LevelGeom& gf, const LevelGeom& gc, const T* res, T* rc, T* xc,
+__device__ __forceinline__ void c_restrict(const LevelGeom gf, const LevelGeom gc, const T* res, T* rc, T* xc,
                                            int tid, int nth) {
     int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
     for (long q = tid; q < gc.npts; q += nth) {
@@ -139,7 +207,7 @@ __device__ __forceinline__ void c_restrict(const LevelGeom& gf, const LevelGeom&
 
 // Same values as k_interp.
 template <class T>
-__device__ __forceinline__ void c_interp(const LevelGeom& gf, const LevelGeom& gc, T* xf, const T* xcv, int tid,
+__device__ __forceinline__ void c_interp(const LevelGeom gf, const LevelGeom gc, T* xf, const T* xcv, int tid,
                                          int nth) {
     for (long q = tid; q < gf.npts; q += nth) {
         int i, j, k;
@@ -187,16 +255,34 @@ __device__ __forceinline__ void c_interp(const LevelGeom& gf, const LevelGeom& g
     }
 }
 
-// x = Minv r on the bottom level, one warp per row (same reduction as k_lu_apply).
+// x = Minv r on the bottom level, one warp per row (same reduction as
+// k_lu_apply).  Levels of up to kLuShared points first gather the source into
+// every CTA's shared memory in natural order, so the row products read it
+// there instead of decoding and loading each entry from L2.
+constexpr int kLuShared = 1024;
+
 template <class T>
-__device__ __forceinline__ void c_lu_apply(const LevelGeom& g, const double* Minv, const T* r, T* x, int tid, int nth) {
+__device__ __forceinline__ void c_lu_apply(const LevelGeom g, const double* Minv, const T* r, T* x, int tid, int nth,
+                                           double* sh) {
     int n = (int)g.npts;
     int lane = tid & 31;
+    if (n <= kLuShared) {
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+            int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+            sh[c] = (double)__ldcg(r + g.ri(i, j, k));
+        }
+        __syncthreads();
+    }
     for (int row = tid >> 5; row < n; row += nth >> 5) {
         double s = 0.0;
-        for (int c = lane; c < n; c += 32) {
-            int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
-            s = fma(Minv[(long)row * n + c], (double)__ldcg(r + g.ri(i, j, k)), s);
+        if (n <= kLuShared) {
+            const double* Mr = Minv + (long)row * n;
+            for (int c = lane; c < n; c += 32) s = fma(__ldg(Mr + c), sh[c], s);
+        } else {
+            for (int c = lane; c < n; c += 32) {
+                int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;
+                s = fma(Minv[(long)row * n + c], (double)__ldcg(r + g.ri(i, j, k)), s);
+            }
         }
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) {
@@ -215,6 +301,7 @@ template <class T>
 __global__ void __launch_bounds__(512) k_coarse_cycle(const CoarsePlan<T>* __restrict__ plans,
                                                       const int* __restrict__ slot_of_cluster,
                                                       const int* __restrict__ active, int mode) {
+    pdl_enter();
     cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
     int csize = (int)cl.num_blocks();
     int cid = blockIdx.x / csize;
@@ -235,7 +322,8 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(const CoarsePlan<T>* __res
     }
     int lb = nl - 1;
     if (P.lu_ok) {
-        c_lu_apply<T>(P.g[lb], P.Minv, P.r[lb], P.x[lb], tid, nth);
+        __shared__ double sh_src[kLuShared];
+        c_lu_apply<T>(P.g[lb], P.Minv, P.r[lb], P.x[lb], tid, nth, sh_src);
         cluster_sync();
     } else {
         c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, P.slab_budget, tid, nth);

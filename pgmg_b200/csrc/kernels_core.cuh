@@ -53,6 +53,7 @@ __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* 
 template <class T, bool EXACT>
 __global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
                                                       const T* __restrict__ A, int col, int k2lo, int k2hi) {
+    pdl_enter();
     long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (p >= (long)k2hi * g.M2 * g.N2) return;
     gs_colour_at<T>(g, x, r, A, col, p);
@@ -99,6 +100,7 @@ __device__ __forceinline__ bool plane_point(const LevelGeom& g, const Plane& P, 
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_gs_plane(LevelGeom g, T* x, const T* __restrict__ r,
                                                      const T* __restrict__ A, int t, Plane P) {
+    pdl_enter();
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     if (!plane_point(g, P, t, w, i, j, k)) return;
@@ -123,6 +125,7 @@ __global__ void __launch_bounds__(kBlock) k_gs_plane(LevelGeom g, T* x, const T*
 template <class T>
 __global__ void __launch_bounds__(1024) k_gs_lex_block(LevelGeom g, T* x, const T* __restrict__ r,
                                                        const T* __restrict__ A, int sweeps, int mode) {
+    pdl_enter();
     int np = num_planes(g);
     for (int s = 0; s < sweeps; s++) {
         for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
@@ -158,6 +161,7 @@ template <class T>
 __global__ void __launch_bounds__(1024) k_gs_mc8_block(LevelGeom g, T* x, const T* __restrict__ r,
                                                        const T* __restrict__ A, int sweeps, int mode,
                                                        long long slab_budget) {
+    pdl_enter();
     int S = slab_count(g, (int)sizeof(T), slab_budget);
     for (int s = 0; s < sweeps; s++) {
         for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
@@ -246,6 +250,7 @@ template <class T, class TO, bool EXACT>
 __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __restrict__ x,
                                                      const T* __restrict__ r, const T* __restrict__ A,
                                                      TO* __restrict__ out, double* __restrict__ partials) {
+    pdl_enter();
     __shared__ double sh[64];
     double s_res = 0, s_rhs = 0;
     residual_at<T, TO>(g, x, r, A, out, blockIdx.y, blockIdx.x * (long)blockDim.x + threadIdx.x, s_res, s_rhs);
@@ -265,6 +270,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __res
 template <class T, class TO>
 __global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restrict__ r, TO* __restrict__ out,
                                                    double* __restrict__ partials) {
+    pdl_enter();
     __shared__ double sh[64];
     int col = blockIdx.y;
     long nc = (long)g.M2 * g.N2 * g.O2;
@@ -287,6 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restr
 // Sums nb partial pairs in a fixed order into out[0], out[1].
 static __global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partials, long nb,
                                                           double* __restrict__ out) {
+    pdl_enter();
     __shared__ double sh[64];
     double a = 0, b = 0;
     for (long q = threadIdx.x; q < nb; q += blockDim.x) { a += partials[2 * q]; b += partials[2 * q + 1]; }
@@ -345,6 +352,7 @@ __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
                                                      T* __restrict__ rc, T* __restrict__ xc) {
+    pdl_enter();
     restrict_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
@@ -405,6 +413,7 @@ __device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& 
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
                                                    const T* __restrict__ xcv) {
+    pdl_enter();
     interp_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
@@ -479,6 +488,7 @@ __global__ void __launch_bounds__(kBlock) k_cm_to_coef(LevelGeom g, const T* __r
 // Interior of x set to zero (region::clear_x_field, region.cc:1679-1682).
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_clear_x(LevelGeom g, T* __restrict__ x) {
+    pdl_enter();
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
     int i, j, k;
@@ -535,6 +545,7 @@ __global__ void __launch_bounds__(kBlock) k_cast(const TI* __restrict__ in, TO* 
 // x64 += x32 over the interior (FP64 update of iterative refinement).
 static __global__ void __launch_bounds__(kBlock) k_add_correction(LevelGeom g, double* __restrict__ x64,
                                                            const float* __restrict__ e32) {
+    pdl_enter();
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
     int i, j, k;

@@ -266,6 +266,7 @@ static __global__ void __launch_bounds__(128) k_lu_inverse(const double* __restr
 template <class T>
 static __global__ void __launch_bounds__(256) k_lu_apply(LevelGeom g, const double* __restrict__ Minv,
                                                   const T* __restrict__ r, T* __restrict__ x) {
+    pdl_enter();
     int n = (int)g.npts;
     int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int l = threadIdx.x & 31;
@@ -290,6 +291,7 @@ template <class T>
 static __global__ void __launch_bounds__(1024) k_lu_solve_exact(LevelGeom g, const double* __restrict__ M,
                                                          const int* __restrict__ piv, const T* __restrict__ r,
                                                          T* __restrict__ x, double* __restrict__ b) {
+    pdl_enter();
     int n = (int)g.npts;
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
         int i = c % g.m, t = c / g.m, j = t % g.n, k = t / g.n;

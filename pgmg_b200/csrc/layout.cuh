@@ -194,6 +194,20 @@ __device__ __forceinline__ void st_keep(float* a, float v, uint64_t pol) {
     asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may be scheduled while the kernel before it
+// in the stream is still draining; it must not touch global memory before
+// pdl_wait() returns (every prerequisite grid complete, its writes visible).
+// pdl_trigger() lets the next such kernel be scheduled.  Both do nothing in a
+// kernel launched without the attribute.  Every kernel of the V-cycle and of
+// the solve loops starts with both calls.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+    pdl_wait();
+    pdl_trigger();
+}
+
 // Offset of slot q in the halo'd x array.
 __host__ __device__ inline long slot_off(const LevelGeom& g, int q) {
     int di = q % 3 - 1, dj = (q / 3) % 3 - 1, dk = q / 9 - 1;
