@@ -92,7 +92,6 @@ void carve(pgmg_handle* h) {
         h->piv = a.take<int>(n);
     }
     h->info = a.take<int>(4);
-    h->lu_scratch = a.take<double>(64);
     h->plan64 = a.take<CoarsePlan<double>>(1);
     h->plan32 = a.take<CoarsePlan<float>>(1);
     h->partials = a.take<double>(2 * maxblocks);
@@ -292,29 +291,6 @@ int probe_cluster(int size) {
     return n;
 }
 
-int probe_lu_cluster(int size) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(size, 1, 1);
-    cfg.blockDim = dim3(512, 1, 1);
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = size;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (size > 8 && cudaFuncSetAttribute(k_lu_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    int nc = 0;
-    if (cudaOccupancyMaxActiveClusters(&nc, k_lu_cluster, &cfg) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return nc;
-}
-
 // One V-cycle (multigrid::v_cycle, multigrid.cc:88-106).  With the 8-colour
 // smoother the levels from h->coarse_first down run as one cluster kernel;
 // the LU-exact coarse solve and the lexicographic smoother use the grid
@@ -426,31 +402,11 @@ pgmg_status lu_setup(pgmg_handle* h) {
     CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 4, h->stream));
     k_lu_build<<<nblk(n * 27), kBlock, 0, h->stream>>>(L.g, L.A64, h->M);
     CKL();
-    if (h->cluster_size > 0) {
-        // One cluster kernel for the whole factorisation.
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(h->cluster_size, 1, 1);
-        cfg.blockDim = dim3(512, 1, 1);
-        cfg.stream = h->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = h->cluster_size;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        CK(cudaLaunchKernelEx(&cfg, k_lu_cluster, h->M, (int)n, h->piv, h->info, h->lu_scratch));
-        h->launches++;
-    } else {
-        for (int j = 0; j < n; j++) {
-            k_lu_pivot<<<1, 1024, 0, h->stream>>>(h->M, (int)n, j, h->piv, h->info);
-            CKL();
-            long rem = n - j - 1;
-            if (rem > 0) {
-                k_lu_update<<<nblk(rem * rem), kBlock, 0, h->stream>>>(h->M, (int)n, j);
-                CKL();
-            }
-        }
+    {
+        // Bandwidth of the 27-point stencil in natural order.
+        int kb = 1 + L.g.m + L.g.m * L.g.n;
+        k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
+        CKL();
     }
     int info = 0;
     double u0 = 0, un = 0;
@@ -462,7 +418,7 @@ pgmg_status lu_setup(pgmg_handle* h) {
     double hi = fabs(u0), lo = fabs(un);
     if (info != 0 || hi == 0 || lo / hi < 2.220446049250313e-16 * 1e4) return PGMG_OK;
     if (h->dims.coarse == PGMG_COARSE_LU) {
-        k_lu_inverse<<<nblk(n, 128), 128, 0, h->stream>>>(h->M, h->piv, (int)n, h->Minv);
+        k_lu_inverse<<<(unsigned)n, 256, n * sizeof(double), h->stream>>>(h->M, h->piv, (int)n, h->Minv);
         CKL();
     }
     h->lu_ok = 1;
@@ -557,7 +513,7 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     }
     h->stream = h->own;
     for (int size : {16, 8}) {
-        if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0 && probe_lu_cluster(size) > 0) {
+        if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0) {
             h->cluster_size = size;
             break;
         }

@@ -85,7 +85,6 @@ struct pgmg_handle {
     double* partials = nullptr;
     double* norm_dev = nullptr;
     double norm_host[2] = {0, 0};
-    double* lu_scratch = nullptr;  // cluster LU pivot candidates
     bool own_arena = true;         // false: memory given by the caller
     // mg_guide state (multigrid.hh:34-118)
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;

@@ -162,101 +162,45 @@ static __global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, dou
     M[row + g.pi(ii, jj, kk) * n] = A[g.ai(i, j, k, s)];
 }
 
-// Column j of the LU factorisation with partial pivoting, the same
-// operations as DGETF2 (and the oracle's restatement): pivot = first row of
-// largest |a_ij|, i >= j; swap rows across the whole matrix; scale the
-// sub-column by 1/a_jj.  info[0] = first zero pivot (1-based).  One block.
-static __global__ void __launch_bounds__(1024) k_lu_pivot(double* __restrict__ M, int n, int j, int* __restrict__ piv,
-                                                   int* __restrict__ info) {
-    __shared__ double sv[32];
-    __shared__ int si[32];
-    __shared__ int sp;
-    double best = -1.0;
-    int bi = n;
-    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
-        double v = fabs(M[i + (long)j * n]);
-        if (v > best) { best = v; bi = i; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        double ov = __shfl_down_sync(0xffffffffu, best, o);
-        int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-    }
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { sv[w] = best; si[w] = bi; }
-    __syncthreads();
-    if (w == 0) {
-        int nw = blockDim.x >> 5;
-        best = l < nw ? sv[l] : -1.0;
-        bi = l < nw ? si[l] : n;
-        for (int o = 16; o > 0; o >>= 1) {
-            double ov = __shfl_down_sync(0xffffffffu, best, o);
-            int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        if (l == 0) sp = bi;
-    }
-    __syncthreads();
-    int p = sp < n ? sp : j;  // all-NaN column: keep the diagonal
-    if (threadIdx.x == 0) piv[j] = p + 1;
-    double apj = M[p + (long)j * n];
-    if (apj != 0.0) {
-        if (p != j)
-            for (int c = threadIdx.x; c < n; c += blockDim.x) {
-                double tmp = M[j + (long)c * n];
-                M[j + (long)c * n] = M[p + (long)c * n];
-                M[p + (long)c * n] = tmp;
-            }
-        __syncthreads();
-        double r = 1.0 / M[j + (long)j * n];
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i + (long)j * n] = __dmul_rn(M[i + (long)j * n], r);
-    } else if (threadIdx.x == 0 && info[0] == 0) {
-        info[0] = j + 1;
-    }
-}
-
-// Rank-1 update of the trailing block after column j.  Thread per element.
-static __global__ void __launch_bounds__(256) k_lu_update(double* __restrict__ M, int n, int j) {
-    long rem = n - j - 1;
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (q >= rem * rem) return;
-    int i = j + 1 + (int)(q % rem);
-    int k = j + 1 + (int)(q / rem);
-    double u = M[j + (long)k * n];
-    if (u != 0.0) M[i + (long)k * n] = __dsub_rn(M[i + (long)k * n], __dmul_rn(M[i + (long)j * n], u));
-}
-
-// Inverse from the factors, row-major Minv[i*n + c]: thread c solves
-// A x = e_c with the recorded interchanges, unit-lower forward and upper
-// backward substitution (column-oriented, as DGETRS), working in column c
-// of the output so that a warp's accesses are contiguous.
-static __global__ void __launch_bounds__(128) k_lu_inverse(const double* __restrict__ M, const int* __restrict__ piv,
+// Explicit inverse from the factors: column c of Minv (row-major) solves
+// A x = e_c as P e_c, then L y = b and U x = y, column-oriented.  One thread
+// block per column, the vector in shared memory; at step j every entry below
+// (forward) or above (backward) j is updated in parallel, each entry
+// receiving the same sequence of operations, in the same order, as a
+// sequential column solve would apply -- so the result does not depend on
+// the block size.
+static __global__ void __launch_bounds__(256) k_lu_inverse(const double* __restrict__ M, const int* __restrict__ piv,
                                                     int n, double* __restrict__ Minv) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    for (int i = 0; i < n; i++) Minv[(long)i * n + c] = (i == c) ? 1.0 : 0.0;
-    for (int i = 0; i < n; i++) {
-        int p = piv[i] - 1;
-        if (p != i) {
-            double t = Minv[(long)i * n + c];
-            Minv[(long)i * n + c] = Minv[(long)p * n + c];
-            Minv[(long)p * n + c] = t;
+    extern __shared__ double X[];
+    int c = blockIdx.x;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) X[i] = (i == c) ? 1.0 : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < n; i++) {
+            int p = piv[i] - 1;
+            if (p != i) {
+                double t = X[i];
+                X[i] = X[p];
+                X[p] = t;
+            }
         }
-    }
+    __syncthreads();
     for (int j = 0; j < n; j++) {
-        double xj = Minv[(long)j * n + c];
+        double xj = X[j];
         if (xj != 0.0)
-            for (int i = j + 1; i < n; i++)
-                Minv[(long)i * n + c] = __dsub_rn(Minv[(long)i * n + c], __dmul_rn(xj, M[i + (long)j * n]));
+            for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+                X[i] = __dsub_rn(X[i], __dmul_rn(xj, M[i + (long)j * n]));
+        __syncthreads();
     }
     for (int j = n - 1; j >= 0; j--) {
-        double xj = Minv[(long)j * n + c];
+        double xj = X[j];
         if (xj != 0.0) {
             xj = xj / M[j + (long)j * n];
-            Minv[(long)j * n + c] = xj;
-            for (int i = 0; i < j; i++)
-                Minv[(long)i * n + c] = __dsub_rn(Minv[(long)i * n + c], __dmul_rn(xj, M[i + (long)j * n]));
+            for (int i = threadIdx.x; i < j; i += blockDim.x)
+                X[i] = __dsub_rn(X[i], __dmul_rn(xj, M[i + (long)j * n]));
         }
+        if (threadIdx.x == 0) Minv[(long)j * n + c] = xj;
+        __syncthreads();
     }
 }
 
@@ -420,62 +364,79 @@ __device__ __forceinline__ void lu_better(double v, int i, double& bv, int& bi) 
     if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
 }
 
-static __global__ void __launch_bounds__(512) k_lu_cluster(double* M, int n, int* __restrict__ piv, int* __restrict__ info,
-                                                    double* scratch) {
-    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-    int ncta = (int)cl.num_blocks();
-    int rank = (int)cl.block_rank();
-    int nth = ncta * blockDim.x;
-    int tid = rank * blockDim.x + threadIdx.x;
-    __shared__ double sv[32];
-    __shared__ int si[32];
+// Partial-pivoting LU (DGETF2 order: idamax pivot, row interchange over all
+// columns, scaling by the reciprocal pivot, rank-1 update skipping zero
+// pivot-row entries) of the coarsest level's dense column-major matrix, in
+// one thread block.  The 27-point stencil in natural order gives the matrix
+// lower and upper bandwidth kl = ku = 1 + m + m*n; with row interchanges the
+// multipliers of column j stay in rows j+1..j+kl and the pivot row in
+// columns up to j+kl+ku, so the pivot search, scaling and update run over
+// that window only.  Entries outside it are zero and a dense factorisation
+// would leave them zero, so the factors are the dense ones bit for bit.
+constexpr int kLuBandMax = 2048;
+
+static __global__ void __launch_bounds__(1024) k_lu_band(double* __restrict__ M, int n, int kl, int ku,
+                                                  int* __restrict__ piv, int* __restrict__ info) {
+    __shared__ double sL[kLuBandMax];
+    __shared__ double sU[kLuBandMax];
+    __shared__ double wv[32];
+    __shared__ int wi[32];
+    __shared__ int s_p;
+    int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
     if (tid == 0) info[0] = 0;
     for (int j = 0; j < n; j++) {
+        int R = min(n - 1, j + kl) - j;       // rows below the diagonal that can be non-zero
+        int C = min(n - 1, j + kl + ku) - j;  // columns right of it in the pivot row
+        // Pivot: first row of largest |M(i,j)|, i = j..j+R.
         double bv = -1.0;
         int bi = n;
-        for (int i = j + tid; i < n; i += nth) lu_better(fabs(__ldcg(M + i + (long)j * n)), i, bv, bi);
+        for (int i = j + tid; i <= j + R; i += blockDim.x) lu_better(fabs(M[i + (long)j * n]), i, bv, bi);
         for (int o = 16; o > 0; o >>= 1) {
             double ov = __shfl_down_sync(0xffffffffu, bv, o);
             int oi = __shfl_down_sync(0xffffffffu, bi, o);
             lu_better(ov, oi, bv, bi);
         }
-        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0) { sv[w] = bv; si[w] = bi; }
+        if (lane == 0) { wv[w] = bv; wi[w] = bi; }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int q = 1; q < (int)(blockDim.x >> 5); q++) lu_better(sv[q], si[q], sv[0], si[0]);
-            scratch[2 * rank] = sv[0];
-            scratch[2 * rank + 1] = (double)si[0];
+        if (tid == 0) {
+            for (int q = 1; q < nw; q++) lu_better(wv[q], wi[q], wv[0], wi[0]);
+            int p = wi[0] < n ? wi[0] : j;
+            s_p = p;
+            piv[j] = p + 1;
         }
-        cl.sync();
-        bv = -1.0;
-        bi = n;
-        for (int c = 0; c < ncta; c++) lu_better(__ldcg(scratch + 2 * c), (int)__ldcg(scratch + 2 * c + 1), bv, bi);
-        int p = bi < n ? bi : j;
-        if (tid == 0) piv[j] = p + 1;
-        double apj = __ldcg(M + p + (long)j * n);
+        __syncthreads();
+        int p = s_p;
+        double apj = M[p + (long)j * n];
         if (apj != 0.0) {
             if (p != j)
-                for (int c = tid; c < n; c += nth) {
-                    double a = __ldcg(M + j + (long)c * n), b2 = __ldcg(M + p + (long)c * n);
+                for (int c = tid; c < n; c += blockDim.x) {
+                    double a = M[j + (long)c * n], b2 = M[p + (long)c * n];
                     M[j + (long)c * n] = b2;
                     M[p + (long)c * n] = a;
                 }
-            cl.sync();
-            double r = 1.0 / __ldcg(M + j + (long)j * n);
-            for (int i = j + 1 + tid; i < n; i += nth) M[i + (long)j * n] = __dmul_rn(__ldcg(M + i + (long)j * n), r);
-        } else if (tid == 0 && info[0] == 0) {
-            info[0] = j + 1;
+            __syncthreads();
+            double r = 1.0 / M[j + (long)j * n];
+            for (int i = tid; i < R; i += blockDim.x) {
+                long a = j + 1 + i + (long)j * n;
+                double v = __dmul_rn(M[a], r);
+                M[a] = v;
+                sL[i] = v;
+            }
+        } else {
+            if (tid == 0 && info[0] == 0) info[0] = j + 1;
+            for (int i = tid; i < R; i += blockDim.x) sL[i] = M[j + 1 + i + (long)j * n];
         }
-        cl.sync();
-        long rem = n - j - 1;
-        for (long q = tid; q < rem * rem; q += nth) {
-            int i = j + 1 + (int)(q % rem);
-            int k = j + 1 + (int)(q / rem);
-            double u = __ldcg(M + j + (long)k * n);
-            if (u != 0.0) M[i + (long)k * n] = __dsub_rn(__ldcg(M + i + (long)k * n), __dmul_rn(__ldcg(M + i + (long)j * n), u));
+        for (int k = tid; k < C; k += blockDim.x) sU[k] = M[j + (long)(j + 1 + k) * n];
+        __syncthreads();
+        for (int q = tid; q < R * C; q += blockDim.x) {
+            int ii = q % R, kk = q / R;
+            double u = sU[kk];
+            if (u != 0.0) {
+                long a = (j + 1 + ii) + (long)(j + 1 + kk) * n;
+                M[a] = __dsub_rn(M[a], __dmul_rn(sL[ii], u));
+            }
         }
-        cl.sync();
+        __syncthreads();
     }
 }
 

@@ -148,6 +148,10 @@ class SolveServer:
         self.running = {}  # slot -> (request, resident)
         self.steps = 0
         self.lock = threading.Lock()  # pool and resident table (set-up thread + loop)
+        # Where the time goes: seconds in set-up (set-up thread), in batch
+        # steps and polls (loop), and the number of set-ups and evictions.
+        self.stats = {"setup_s": 0.0, "setups": 0, "step_s": 0.0, "poll_s": 0.0, "start_s": 0.0,
+                      "evictions": 0, "idle_s": 0.0}
 
     # -- resident hierarchies --------------------------------------------------
     def _evict_for(self, nbytes: int):
@@ -169,6 +173,7 @@ class SolveServer:
             r = self.resident.pop(victim)
             r.mg.close()
             self.pool.release(r.off, r.nbytes)
+            self.stats["evictions"] += 1
 
     def _build(self, req: Request, now: float):
         m, n, o = req.shape
@@ -206,7 +211,10 @@ class SolveServer:
                 except queue.Empty:
                     continue
                 try:
-                    r = self._build(req, time.perf_counter() - t0)
+                    ts = time.perf_counter()
+                    r = self._build(req, ts - t0)
+                    self.stats["setup_s"] += time.perf_counter() - ts
+                    self.stats["setups"] += 1
                     ready.put((req, r))
                 except Exception as e:  # noqa: BLE001 -- reported to the caller
                     err.append(e)
@@ -256,10 +264,14 @@ class SolveServer:
                         self.resident[res.pid] = res
                     self._start(req, res, reused=False, now=time.perf_counter() - t0)
                 if self.running:
+                    ts = time.perf_counter()
                     self.batch.step(self.tol, self.max_cycles)
                     self.steps += 1
+                    tp = time.perf_counter()
                     act, cyc, rr = self.batch.poll()
                     now = time.perf_counter() - t0
+                    self.stats["step_s"] += tp - ts
+                    self.stats["poll_s"] += now + t0 - tp
                     for slot in [s for s in self.running if not act[s]]:
                         req, res = self.running.pop(slot)
                         req.finished = now
@@ -277,13 +289,16 @@ class SolveServer:
                         done.append(req)
                 else:
                     nxt = pending[0].arrival - (time.perf_counter() - t0) if pending else 0.0
+                    ts = time.perf_counter()
                     time.sleep(min(max(nxt, 0.0), 0.002))
+                    self.stats["idle_s"] += time.perf_counter() - ts
         finally:
             stop.set()
             worker.join(timeout=5)
         return done
 
     def _start(self, req: Request, res: _Resident, reused: bool, now: float):
+        ts = time.perf_counter()
         slot = self.free_slots.pop()
         with self.lock:
             res.busy = True
@@ -296,6 +311,7 @@ class SolveServer:
         self.batch.attach(slot, res.mg)
         self.batch.begin(slot)
         self.running[slot] = (req, res)
+        self.stats["start_s"] += time.perf_counter() - ts
 
     def close(self):
         for r in self.resident.values():
