@@ -739,7 +739,11 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
         Level& Cl = h->L[l];
         k_rat_bounds<<<nblk(Cl.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, F.S, Cl.S);
         CKL();
-        k_rat_fill<<<nblk(Cl.g.npts, 128), 128, 0, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+        if (Cl.g.npts <= kRatSmallMax)
+            k_rat_fill_small<<<nblk(Cl.g.npts * 32, kRatSmallBlock), kRatSmallBlock, 0, h->stream>>>(F.g, Cl.g, F.A64,
+                                                                                                   F.S, Cl.A64);
+        else
+            k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, 0, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         CKL();
     }
     if (h->dims.precision == PGMG_MIXED)

@@ -71,9 +71,16 @@ static __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGe
 // axis, and A_add (:1173-1180) adds it to this coarse point's row.  Products
 // by powers of two are exact, sums are rounded one by one (no fused
 // multiply-add), so the result matches the reference bit for bit.
-// Grid: one thread per coarse point.  Output: colour-major coarse stencils.
-static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
-                                                  const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
+// Grid: one thread per coarse point.  Each fine point's 27 coefficients are
+// loaded at once into the thread's column of a shared-memory tile (27
+// independent loads, one memory latency) and its ~90 terms read them there.
+// Output: colour-major coarse stencils.
+constexpr int kRatBlock = 128;
+
+static __global__ void __launch_bounds__(kRatBlock, 4) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
+                                                        const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
+    __shared__ double sa[27 * kRatBlock];
+    double* my = sa + threadIdx.x;
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q >= gc.npts) return;
     int I, J, K;
@@ -111,6 +118,8 @@ static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom
                             grid_map(St[4], St[5], gf.o);
                             int fcol = gf.colour(ti, tj, tk);
                             const double* fa = Af + (long)fcol * 27 * gf.Nc + gf.cidx(ti, tj, tk);
+#pragma unroll
+                            for (int u = 0; u < 27; u++) my[u * kRatBlock] = __ldg(fa + u * gf.Nc);
                             for (int vk = St[4]; vk < St[5]; vk++) {
                                 int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
                                 for (int vj = St[2]; vj < St[3]; vj++) {
@@ -124,7 +133,7 @@ static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom
                                                 double jkfac = jj == cj ? kfac : 0.5 * kfac;
                                                 for (int ii = li; ii < ui; ii++) {
                                                     int slot = (ii - ti + 1) + 3 * (jj - tj + 1) + 9 * (kk - tk + 1);
-                                                    double term = __dmul_rn(__dmul_rn(0.125, fa[slot * gf.Nc]),
+                                                    double term = __dmul_rn(__dmul_rn(0.125, my[slot * kRatBlock]),
                                                                             ii == ci ? jkfac : 0.5 * jkfac);
                                                     At = __dadd_rn(At, term);
                                                 }
@@ -145,6 +154,92 @@ static __global__ void __launch_bounds__(128) k_rat_fill(LevelGeom gf, LevelGeom
     long c = gc.cidx(I, J, K);
 #pragma unroll
     for (int s = 0; s < 27; s++) Ac[((long)col * 27 + s) * gc.Nc + c] = acc[s];
+}
+
+// k_rat_fill for small coarse levels, where one thread per coarse point
+// leaves the GPU nearly empty: one warp per coarse point, lane s < 27 owning
+// coarse stencil slot s (neighbour v = (I,J,K) + (s%3-1, s/3%3-1, s/9-1)).
+// The warp walks the fine points in scan order together -- their boxes and
+// factors are the same for every lane; lanes 0..26 first load the fine
+// point's 27 coefficients into the warp's shared row -- and each lane adds
+// the term for its own v, so every accumulator receives its terms in the
+// same order as in k_rat_fill: the results are identical.
+constexpr int kRatSmallBlock = 128;
+constexpr long kRatSmallMax = 20000;  // coarse levels up to this size use the warp form
+
+static __global__ void __launch_bounds__(kRatSmallBlock, 4) k_rat_fill_small(LevelGeom gf, LevelGeom gc,
+                                                                   const double* __restrict__ Af,
+                                                                   const int8_t* __restrict__ Sf,
+                                                                   double* __restrict__ Ac) {
+    __shared__ double srow[kRatSmallBlock / 32][32];
+    long q = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    double* row = srow[threadIdx.x >> 5];
+    if (q >= gc.npts) return;
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
+    const bool mine = lane < 27;
+    const int vi = I + lane % 3 - 1, vj = J + (lane / 3) % 3 - 1, vk = K + lane / 9 - 1;
+    double acc = 0.0;
+    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    for (int cz = K - 1; cz <= K; cz++) {
+        if (cz < 0 || cz > lz) continue;
+        for (int cy = J - 1; cy <= J; cy++) {
+            if (cy < 0 || cy > ly) continue;
+            for (int cx = I - 1; cx <= I; cx++) {
+                if (cx < 0 || cx > lx) continue;
+                for (int dz = 0; dz < 2; dz++) {
+                    if (dz && !has_upper(cz, gf.o)) continue;
+                    bool zsn = snapped(cz, gf.o);
+                    if (tweight(cz, dz, K, zsn) == 0.0) continue;
+                    for (int dy = 0; dy < 2; dy++) {
+                        if (dy && !has_upper(cy, gf.n)) continue;
+                        bool ysn = snapped(cy, gf.n);
+                        if (tweight(cy, dy, J, ysn) == 0.0) continue;
+                        for (int dx = 0; dx < 2; dx++) {
+                            if (dx && !has_upper(cx, gf.m)) continue;
+                            bool xsn = snapped(cx, gf.m);
+                            if (tweight(cx, dx, I, xsn) == 0.0) continue;
+                            double fac = ((dx && !xsn) ? 0.5 : 1.0) * ((dy && !ysn) ? 0.5 : 1.0) *
+                                         ((dz && !zsn) ? 0.5 : 1.0);
+                            int ti = 2 * cx + dx, tj = 2 * cy + dy, tk = 2 * cz + dz;
+                            const double* fa = Af + (long)gf.colour(ti, tj, tk) * 27 * gf.Nc + gf.cidx(ti, tj, tk);
+                            __syncwarp();
+                            if (mine) row[lane] = __ldg(fa + lane * gf.Nc);
+                            __syncwarp();
+                            const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                            int B[6] = {fs[0] + ti, fs[1] + ti, fs[2] + tj, fs[3] + tj, fs[4] + tk, fs[5] + tk};
+                            int St[6] = {B[0], B[1], B[2], B[3], B[4], B[5]};
+                            grid_map(St[0], St[1], gf.m);
+                            grid_map(St[2], St[3], gf.n);
+                            grid_map(St[4], St[5], gf.o);
+                            if (!mine || vi < St[0] || vi >= St[1] || vj < St[2] || vj >= St[3] || vk < St[4] ||
+                                vk >= St[5])
+                                continue;
+                            int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
+                            int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n);
+                            int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m);
+                            double At = 0.0;
+                            for (int kk = lk; kk < uk; kk++) {
+                                double kfac = kk == ck ? 1.0 : 0.5;
+                                for (int jj = lj; jj < uj; jj++) {
+                                    double jkfac = jj == cj ? kfac : 0.5 * kfac;
+                                    for (int ii = li; ii < ui; ii++) {
+                                        int slot = (ii - ti + 1) + 3 * (jj - tj + 1) + 9 * (kk - tk + 1);
+                                        double term = __dmul_rn(__dmul_rn(0.125, row[slot]),
+                                                                ii == ci ? jkfac : 0.5 * jkfac);
+                                        At = __dadd_rn(At, term);
+                                    }
+                                }
+                            }
+                            acc = __dadd_rn(acc, __dmul_rn(At, fac));
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (mine) Ac[((long)gc.colour(I, J, K) * 27 + lane) * gc.Nc + gc.cidx(I, J, K)] = acc;
 }
 
 // ---------------------------------------------------------------------------

@@ -106,17 +106,19 @@ class FieldPool:
         self.device = device
         self.width = width
         self.fields = {}
+        self.lock = threading.Lock()
 
     def get(self, shape, fid: int):
         key = (tuple(shape), fid)
-        if key not in self.fields:
-            import torch
-            m, n, o = shape
-            g = problem_gauss(m, n, o, 1000 + 7919 * fid + 31 * m + 17 * n + o, self.width)
-            t = torch.from_numpy(g).to(f"cuda:{self.device}")
-            torch.cuda.synchronize(self.device)
-            self.fields[key] = t
-        return self.fields[key]
+        with self.lock:
+            if key not in self.fields:
+                import torch
+                m, n, o = shape
+                g = problem_gauss(m, n, o, 1000 + 7919 * fid + 31 * m + 17 * n + o, self.width)
+                t = torch.from_numpy(g).to(f"cuda:{self.device}")
+                torch.cuda.synchronize(self.device)
+                self.fields[key] = t
+            return self.fields[key]
 
 
 class _Resident:
@@ -125,14 +127,15 @@ class _Resident:
         self.mg = mg
         self.off = off
         self.nbytes = nbytes
-        self.busy = False
+        self.busy = True  # built for a request that is about to start
         self.slot = -1
         self.last_used = 0.0
 
 
 class SolveServer:
     def __init__(self, cap_bytes: float, max_slots: int = 64, precision: int = MIXED, tol: float = 1e-10,
-                 max_cycles: int = 100, device: int = 0, keep_solutions: bool = False, fields: FieldPool | None = None):
+                 max_cycles: int = 100, device: int = 0, keep_solutions: bool = False, fields: FieldPool | None = None,
+                 setup_threads: int = 4):
         self.cap = int(cap_bytes)
         self.max_slots = max_slots
         self.precision = precision
@@ -140,6 +143,10 @@ class SolveServer:
         self.max_cycles = max_cycles
         self.device = device
         self.keep = keep_solutions
+        # Set-up threads: each builds one problem at a time on that problem's
+        # own stream, so the set-up kernels of several problems (the coarse LU
+        # is one thread block) overlap each other and the batch steps.
+        self.setup_threads = max(1, int(setup_threads))
         self.pool = DevicePool(self.cap, device)
         self.fields = fields or FieldPool(device)
         self.batch = Batch(max_slots, precision, device)
@@ -213,15 +220,18 @@ class SolveServer:
                 try:
                     ts = time.perf_counter()
                     r = self._build(req, ts - t0)
-                    self.stats["setup_s"] += time.perf_counter() - ts
-                    self.stats["setups"] += 1
+                    with self.lock:
+                        self.stats["setup_s"] += time.perf_counter() - ts
+                        self.stats["setups"] += 1
                     ready.put((req, r))
                 except Exception as e:  # noqa: BLE001 -- reported to the caller
                     err.append(e)
                     ready.put((req, None))
 
-        worker = threading.Thread(target=setup_worker, daemon=True)
-        worker.start()
+        workers = [threading.Thread(target=setup_worker, daemon=True) for _ in range(self.setup_threads)]
+        for w in workers:
+            w.start()
+        max_in_setup = 2 * self.setup_threads
         in_setup = 0
         total = len(pending)
         try:
@@ -235,10 +245,15 @@ class SolveServer:
                 while waiting:
                     req = waiting.popleft()
                     with self.lock:
+                        # Claim an idle resident hierarchy before a set-up
+                        # thread can pick it for eviction.
                         res = self.resident.get(req.problem)
-                    if res is not None and not res.busy and self.free_slots:
+                        reuse = res is not None and not res.busy and bool(self.free_slots)
+                        if reuse:
+                            res.busy = True
+                    if reuse:
                         self._start(req, res, reused=True, now=now)
-                    elif res is None and req.problem not in building and in_setup < 4 and \
+                    elif res is None and req.problem not in building and in_setup < max_in_setup and \
                             len(self.free_slots) > in_setup:
                         building.add(req.problem)
                         in_setup += 1
@@ -294,7 +309,8 @@ class SolveServer:
                     self.stats["idle_s"] += time.perf_counter() - ts
         finally:
             stop.set()
-            worker.join(timeout=5)
+            for w in workers:
+                w.join(timeout=5)
         return done
 
     def _start(self, req: Request, res: _Resident, reused: bool, now: float):
