@@ -82,18 +82,34 @@ class Clocks:
         self.proc = None
         self.f = None
 
+    def _lines(self):
+        try:
+            with open(self.f.name) as fh:
+                return sum(1 for _ in fh)
+        except Exception:
+            return 0
+
     def __enter__(self):
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
+            # The timed region starts once the sampler is producing samples.
+            t0 = time.time()
+            while self._lines() < 1 and time.time() - t0 < 10 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.skip = self._lines()
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
+            # Keep it until it has logged the samples taken during the region.
+            t0 = time.time()
+            while self._lines() < self.skip + 2 and time.time() - t0 < 2 and self.proc.poll() is None:
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -106,9 +122,9 @@ class Clocks:
         self.f.flush()
         rows = []
         with open(self.f.name) as fh:
-            for line in fh:
+            for q, line in enumerate(fh):
                 p = [x.strip() for x in line.split(",")]
-                if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                if q >= getattr(self, "skip", 0) and len(p) >= 9 and p[1].replace(".", "").isdigit():
                     rows.append(p)
         os.unlink(self.f.name)
         if not rows:

@@ -661,6 +661,7 @@ pgmg_status pgmg_batch_attach(pgmg_batch* b, int slot, pgmg_handle* h) {
     if (b->slots[slot]) return bfail(b, PGMG_ERR_ARG, "slot %d is occupied", slot);
     if (!h->built) return bfail(b, PGMG_ERR_SETUP, "problem operators not built");
     if (h->dims.precision != b->precision) return bfail(b, PGMG_ERR_ARG, "precision differs from the batch's");
+    if (h->prd) return bfail(b, PGMG_ERR_UNSUPPORTED, "batched problems are non-periodic");
     if (h->dims.smoother != PGMG_SMOOTH_MC8 || h->cluster_size == 0 || h->slab_budget != 0 ||
         h->dims.coarse == PGMG_COARSE_LU_EXACT)
         return bfail(b, PGMG_ERR_UNSUPPORTED, "batched problems use the 8-colour smoother with the cluster coarse cycle");

@@ -48,14 +48,15 @@ pgmg_status fail(pgmg_handle* h, pgmg_status st, const char* fmt, ...) {
     } while (0)
 
 // Hierarchy plan (multigrid::setup_hierarchy, multigrid.cc:17-85; coarse
-// sizes region.cc:14).  Periodic axes are not built yet.
+// sizes region.cc:14: (m+2)>>1, or (m+1)>>1 on a periodic axis).
 int plan_levels(const pgmg_dims& d, LevelGeom* g) {
     int nl = 0;
     int m = d.m, n = d.n, o = d.o;
-    g[nl++] = make_geom(m, n, o);
+    int prd = (d.x_prd ? 1 : 0) | (d.y_prd ? 2 : 0) | (d.z_prd ? 4 : 0);
+    g[nl++] = make_geom(m, n, o, prd);
     while ((long)m * n * o > 1024 && nl < kMaxLevels) {
-        m = (m + 2) >> 1; n = (n + 2) >> 1; o = (o + 2) >> 1;
-        g[nl++] = make_geom(m, n, o);
+        m = (m + (d.x_prd ? 1 : 2)) >> 1; n = (n + (d.y_prd ? 1 : 2)) >> 1; o = (o + (d.z_prd ? 1 : 2)) >> 1;
+        g[nl++] = make_geom(m, n, o, prd);
     }
     return nl;
 }
@@ -119,11 +120,43 @@ template <class T> View<T> view(Level& L);
 template <> View<double> view<double>(Level& L) { return view64(L); }
 template <> View<float> view<float>(Level& L) { return view32(L); }
 
+// Periodic images of a level's solution (no-op on non-periodic levels).
+template <class T>
+pgmg_status wrap_level(pgmg_handle* h, int l) {
+    const LevelGeom& g = h->L[l].g;
+    if (!g.prd) return PGMG_OK;
+    LAUNCH(nblk(halo_cells(g)), kBlock, k_halo_wrap<T>, g, view<T>(h->L[l]).x);
+    return PGMG_OK;
+}
+
 template <class T>
 pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps = 1) {
     Level& L = h->L[l];
     View<T> v = view<T>(L);
     const LevelGeom& g = L.g;
+    // An odd periodic axis (possible on the bottom level only) has no valid
+    // 8-colouring: sweep that level lexicographically.
+    if (g.prd && ((px(g) && (g.m & 1)) || (py(g) && (g.n & 1)) || (pz(g) && (g.o & 1))))
+        smoother = PGMG_SMOOTH_LEX;
+    if (smoother == PGMG_SMOOTH_LEX && g.prd) {
+        // region::gauss_seidel (region.cc:355-361) refreshes the ghosts once
+        // per call and sweeps with them fixed: the images are refreshed
+        // before each sweep (and after the last), and the hyperplane kernel
+        // reads but never writes them.
+        int np = num_planes(g);
+        for (int s = 0; s < sweeps; s++) {
+            TRY(wrap_level<T>(h, l));
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int tt = 0; tt < np; tt++) {
+                    int t = pass ? np - 1 - tt : tt;
+                    Plane P = plane_range(g, t);
+                    long nw = (long)(P.kmax - P.kmin + 1) * P.jw;
+                    if (nw <= 0) continue;
+                    LAUNCH(nblk(nw), kBlock, k_gs_plane<T>, g, v.x, v.r, v.A, t, P);
+                }
+        }
+        return wrap_level<T>(h, l);
+    }
     if (smoother == PGMG_SMOOTH_LEX) {
         if (g.npts <= kLexBlockMax) {
             LAUNCH(1, 1024, k_gs_lex_block<T>, g, v.x, v.r, v.A, sweeps, mode);
@@ -141,7 +174,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 }
         return PGMG_OK;
     }
-    if (g.npts <= kMc8BlockMax) {
+    if (g.npts <= kMc8BlockMax && !g.prd) {
         LAUNCH(1, 1024, k_gs_mc8_block<T>, g, v.x, v.r, v.A, sweeps, mode, h->slab_budget);
         return PGMG_OK;
     }
@@ -177,7 +210,7 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     View<T> vf = view<T>(F), vc = view<T>(Cl);
     TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
     LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
-    return PGMG_OK;
+    return wrap_level<T>(h, l);
 }
 
 template <class T>
@@ -185,7 +218,7 @@ pgmg_status interp_level(pgmg_handle* h, int l) {
     Level& F = h->L[l - 1];
     Level& Cl = h->L[l];
     LAUNCH(nblk(F.g.npts), kBlock, k_interp<T>, F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
-    return PGMG_OK;
+    return wrap_level<T>(h, l - 1);
 }
 
 template <class T>
@@ -200,7 +233,7 @@ pgmg_status coarse_solve_t(pgmg_handle* h, int smoother) {
             long thr = L.g.npts * 32;
             LAUNCH(nblk(thr), kBlock, k_lu_apply<T>, L.g, h->Minv, v.r, v.x);
         }
-        return PGMG_OK;
+        return wrap_level<T>(h, lb);
     }
     // region::solve_exact fallback: pgmg_gs_exact plain (mode 0) sweeps of
     // the cycle's smoother (region_tr.cc:557; the reference's own smoother is
@@ -387,8 +420,10 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
         if (rhs2) *rhs2 = h->norm_host[1];
     }
     LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
+    TRY(wrap_level<float>(h, 0));
     TRY(run_vcycle<float>(h, mode, smoother));
     LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+    TRY(wrap_level<double>(h, 0));
     return PGMG_OK;
 }
 
@@ -400,11 +435,13 @@ pgmg_status lu_setup(pgmg_handle* h) {
     if (n >= kMaxExact || h->dims.coarse == PGMG_COARSE_GS) return PGMG_OK;
     CK(cudaMemsetAsync(h->M, 0, sizeof(double) * n * n, h->stream));
     CK(cudaMemsetAsync(h->info, 0, sizeof(int) * 4, h->stream));
-    k_lu_build<<<nblk(n * 27), kBlock, 0, h->stream>>>(L.g, L.A64, h->M);
+    k_lu_build<<<nblk(n), kBlock, 0, h->stream>>>(L.g, L.A64, L.S, h->M);
     CKL();
     {
-        // Bandwidth of the 27-point stencil in natural order.
-        int kb = 1 + L.g.m + L.g.m * L.g.n;
+        // Bandwidth of the 27-point stencil in natural order (a periodic
+        // axis couples the first and last planes: no band).
+        int kb = L.g.prd ? (int)n - 1 : 1 + L.g.m + L.g.m * L.g.n;
+        if (kb > (int)n - 1) kb = (int)n - 1;
         k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
         CKL();
     }
@@ -469,7 +506,6 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     if (!dims || !out) return PGMG_ERR_ARG;
     *out = nullptr;
     if (dims->m < 2 || dims->n < 2 || dims->o < 2) return PGMG_ERR_ARG;
-    if (dims->x_prd || dims->y_prd || dims->z_prd) return PGMG_ERR_UNSUPPORTED;
     if (dims->precision != PGMG_FP64 && dims->precision != PGMG_MIXED) return PGMG_ERR_ARG;
     if (dims->coarse < PGMG_COARSE_LU || dims->coarse > PGMG_COARSE_LU_EXACT) return PGMG_ERR_ARG;
     int ndev = 0;
@@ -487,6 +523,16 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     LevelGeom g[kMaxLevels];
     h->nl = plan_levels(*dims, g);
     for (int l = 0; l < h->nl; l++) h->L[l].g = g[l];
+    h->prd = g[0].prd;
+    // Periodic axes: every level that is smoothed and restricted (all but
+    // the bottom) must be even along them -- the 8-colour order needs the
+    // wrap-around neighbours to differ in parity, and the transfers here
+    // cover even periodic axes (coarse size m/2).
+    for (int l = 0; l + 1 < h->nl; l++)
+        if ((px(g[l]) && (g[l].m & 1)) || (py(g[l]) && (g[l].n & 1)) || (pz(g[l]) && (g[l].o & 1))) {
+            delete h;
+            return PGMG_ERR_UNSUPPORTED;
+        }
     carve(h);  // count
     size_t bytes = h->arena.used;
     if (mem) {
@@ -521,6 +567,12 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     h->coarse_first = h->nl - 1;
     for (int l = 0; l < h->nl; l++)
         if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
+    if (h->prd) {
+        // Periodic levels keep their halo images current between kernels
+        // (k_halo_wrap), so they run with the per-level kernels only.
+        h->cluster_size = 0;
+        h->coarse_first = h->nl;
+    }
     if (cudaMemsetAsync(h->arena.base, 0, bytes, h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess) {
         pgmg_dev_destroy(h);
@@ -579,6 +631,7 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             break;
         case PGMG_OPT_CLUSTER_SIZE:
             if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
+            if (value && h->prd) return fail(h, PGMG_ERR_UNSUPPORTED, "periodic problems run without the cluster coarse cycle");
             if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
                 return fail(h, PGMG_ERR_UNSUPPORTED, "cluster of %lld CTAs not launchable", value);
             h->cluster_size = (int)value;
@@ -665,7 +718,7 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
                 int lo = b[2 * a], hi = b[2 * a + 1];
                 if (lo < -1 || hi > 2 || lo >= hi || lo > 0 || hi < 1)
                     return fail(h, PGMG_ERR_ARG, "box of point (%d,%d,%d) axis %d is [%d,%d): must contain 0 and lie in [-1,2)", i, j, k, a, lo, hi);
-                if (c[a] + lo < 0 || c[a] + hi > ext[a])
+                if (!((h->prd >> a) & 1) && (c[a] + lo < 0 || c[a] + hi > ext[a]))
                     return fail(h, PGMG_ERR_ARG, "box of point (%d,%d,%d) leaves the non-periodic grid on axis %d", i, j, k, a);
                 s8[6 * p + 2 * a] = (int8_t)lo;
                 s8[6 * p + 2 * a + 1] = (int8_t)hi;
@@ -676,8 +729,9 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
             int i = (int)(p % g.m), j = (int)((p / g.m) % g.n), k = (int)(p / ((long)g.m * g.n));
             int c[3] = {i, j, k}, ext[3] = {g.m, g.n, g.o};
             for (int a = 0; a < 3; a++) {
-                s8[6 * p + 2 * a] = (int8_t)(c[a] > 0 ? -1 : 0);
-                s8[6 * p + 2 * a + 1] = (int8_t)(c[a] < ext[a] - 1 ? 2 : 1);
+                bool pa = (h->prd >> a) & 1;
+                s8[6 * p + 2 * a] = (int8_t)(pa || c[a] > 0 ? -1 : 0);
+                s8[6 * p + 2 * a + 1] = (int8_t)(pa || c[a] < ext[a] - 1 ? 2 : 1);
             }
         }
     }
@@ -701,6 +755,7 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
 
 pgmg_status pgmg_dev_assemble_q1(pgmg_handle* h, const double* cells, int from_log, double sigma) {
     if (!h) return PGMG_ERR_ARG;
+    if (h->prd) return fail(h, PGMG_ERR_UNSUPPORTED, "the Q1 generator builds Dirichlet problems only");
     Level& L = h->L[0];
     const LevelGeom& g = L.g;
     const double* dc = nullptr;
@@ -803,6 +858,7 @@ pgmg_status pgmg_dev_set_field(pgmg_handle* h, int level, int field, const doubl
     if (field == PGMG_FIELD_X) k_nat_to_x<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L.x64);
     else k_nat_to_cm<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L.r64);
     CKL();
+    if (field == PGMG_FIELD_X) TRY(wrap_level<double>(h, level));
     CK(cudaStreamSynchronize(h->stream));
     return PGMG_OK;
 }
@@ -841,7 +897,7 @@ pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
     if (level == 0) h->x0_zero = true;
     LAUNCH(nblk(h->L[level].g.npts), kBlock, k_clear_x<double>, h->L[level].g, h->L[level].x64);
-    return PGMG_OK;
+    return wrap_level<double>(h, level);
 }
 
 pgmg_status pgmg_dev_setup_test(pgmg_handle* h, int level, int ca, int xfield) {
@@ -850,7 +906,7 @@ pgmg_status pgmg_dev_setup_test(pgmg_handle* h, int level, int ca, int xfield) {
     Level& L = h->L[level];
     k_setup_test<double><<<nblk(L.g.npts), kBlock, 0, h->stream>>>(L.g, L.x64, L.r64, ca, xfield);
     CKL();
-    return PGMG_OK;
+    return wrap_level<double>(h, level);
 }
 
 pgmg_status pgmg_dev_gs(pgmg_handle* h, int level, int mode, int smoother) {
@@ -1062,8 +1118,10 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             if (inner > max_cycles - nc) inner = max_cycles - nc;
             if (inner < 1) inner = 1;
             LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
+            TRY(wrap_level<float>(h, 0));
             for (int i = 0; i < inner; i++) TRY(run_vcycle<float>(h, 0, smoother));
             LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+            TRY(wrap_level<double>(h, 0));
             nc += inner;
             continue;
         } else {

@@ -48,6 +48,9 @@ __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* 
     const T* Ap = A + (long)col * 27 * g.Nc + p;
     T v = gs_value<T, true>(g, x, xc, Ap, g.Nc, ld_stream(r + (long)col * g.Nc + p, ps), ps, pk);
     st_keep(x + xc, v, pk);
+    // Periodic axes: the point's images in the halo are updated with it; the
+    // points that read them are of other colours (periodic sizes are even).
+    if (g.prd) store_images<T>(g, x, i, j, k, v);
 }
 
 template <class T, bool EXACT>
@@ -315,28 +318,30 @@ __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom
     if (q >= gc.npts) return;
     int I, J, K;
     decode_nat(gc, q, I, J, K);
-    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     T acc = T(0);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < 0 || cz > lz) continue;
-        bool zsn = snapped(cz, gf.o);
+        if (cz < cube_first(qz) || cz > lz) continue;
+        bool zsn = snapped(cz, gf.o, qz);
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < 0 || cy > ly) continue;
+            if (cy < cube_first(qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < 0 || cx > lx) continue;
-                bool xsn = snapped(cx, gf.m);
+                if (cx < cube_first(qx) || cx > lx) continue;
+                bool xsn = snapped(cx, gf.m, qx);
                 for (int dz = 0; dz < 2; dz++) {
-                    if (dz && !has_upper(cz, gf.o)) continue;
+                    if (dz && !has_upper(cz, gf.o, qz)) continue;
                     double wz = tweight(cz, dz, K, zsn);
                     if (wz == 0.0) continue;
                     for (int dy = 0; dy < 2; dy++) {
-                        if (dy && !has_upper(cy, gf.n)) continue;
+                        if (dy && !has_upper(cy, gf.n, qy)) continue;
                         for (int dx = 0; dx < 2; dx++) {
-                            if (dx && !has_upper(cx, gf.m)) continue;
-                            bool ysn = (!dx && dy && dz) ? xsn : snapped(cy, gf.n);
+                            if (dx && !has_upper(cx, gf.m, qx)) continue;
+                            bool ysn = (!dx && dy && dz) ? xsn : snapped(cy, gf.n, qy);
                             double w = tweight(cx, dx, I, xsn) * tweight(cy, dy, J, ysn) * wz;
                             if (w == 0.0) continue;
-                            int fi = 2 * cx + dx, fj = 2 * cy + dy, fk = 2 * cz + dz;
+                            int fi = wrap(2 * cx + dx, gf.m, qx), fj = wrap(2 * cy + dy, gf.n, qy),
+                                fk = wrap(2 * cz + dz, gf.o, qz);
                             T rd = (T)(0.125 * w) * res[gf.ri(fi, fj, fk)];
                             acc = add_rn<T>(acc, rd);
                         }
@@ -377,7 +382,10 @@ __device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& 
     const T h = T(0.5), qq = T(0.25), e = T(0.125);
     int role = dx | (dy << 1) | (dz << 2);
     T val;
-    bool full = Cx < cube_last(gf.m) && Cy < cube_last(gf.n) && Cz < cube_last(gf.o);
+    // Periodic axes: every cube is full, its upper coarse corner at the last
+    // cube being coarse 0's image in the halo.
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    bool full = (qx || Cx < cube_last(gf.m)) && (qy || Cy < cube_last(gf.n)) && (qz || Cz < cube_last(gf.o));
     if (full) {
         switch (role) {
             case 0: val = v0; break;
@@ -390,7 +398,7 @@ __device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& 
             default: val = e * (((((((v0 + v1) + v2) + v3) + (v4 + v5)) + v6) + v7)); break;
         }
     } else {
-        bool xs = snapped(Cx, gf.m), ys = snapped(Cy, gf.n), zs = snapped(Cz, gf.o);
+        bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
         switch (role) {
             case 0: val = v0; break;
             case 1: val = xs ? v1 : h * (v0 + v1); break;
@@ -483,6 +491,41 @@ __global__ void __launch_bounds__(kBlock) k_cm_to_coef(LevelGeom g, const T* __r
     int s = (int)(q % 27);
     int i = (int)(pt % g.m); long t = pt / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
     dst[q] = (double)A[g.ai(i, j, k, s)];
+}
+
+// Periodic images: every halo cell whose out-of-range coordinates are all
+// on periodic axes takes the value of the interior point it wraps to (the
+// reference's ghost exchange with itself, region.cc:1338-1469, on one
+// process).  Halo cells enumerated face by face: z faces (whole (m+2)x(n+2)
+// planes), then y faces (without z halo rows), then x faces.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_halo_wrap(LevelGeom g, T* __restrict__ x) {
+    pdl_enter();
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long zf = 2L * g.mx * g.my, yf = 2L * g.mx * g.o, xf = 2L * g.n * g.o;
+    int i, j, k;
+    if (q < zf) {
+        long t = q % (g.mx * g.my);
+        i = (int)(t % g.mx) - 1; j = (int)(t / g.mx) - 1; k = q < g.mx * g.my ? -1 : g.o;
+    } else if (q < zf + yf) {
+        long t = q - zf, u = t % (g.mx * g.o);
+        i = (int)(u % g.mx) - 1; k = (int)(u / g.mx); j = t < g.mx * g.o ? -1 : g.n;
+    } else if (q < zf + yf + xf) {
+        long t = q - zf - yf, u = t % ((long)g.n * g.o);
+        j = (int)(u % g.n); k = (int)(u / g.n); i = t < (long)g.n * g.o ? -1 : g.m;
+    } else {
+        return;
+    }
+    bool ox = i < 0 || i >= g.m, oy = j < 0 || j >= g.n, oz = k < 0 || k >= g.o;
+    if ((ox && !px(g)) || (oy && !py(g)) || (oz && !pz(g))) return;
+    int wi = i < 0 ? g.m - 1 : (i >= g.m ? 0 : i);
+    int wj = j < 0 ? g.n - 1 : (j >= g.n ? 0 : j);
+    int wk = k < 0 ? g.o - 1 : (k >= g.o ? 0 : k);
+    x[g.xi(i, j, k)] = x[g.xi(wi, wj, wk)];
+}
+
+__host__ __device__ inline long halo_cells(const LevelGeom& g) {
+    return 2L * g.mx * g.my + 2L * g.mx * g.o + 2L * g.n * g.o;
 }
 
 // Interior of x set to zero (region::clear_x_field, region.cc:1679-1682).

@@ -16,15 +16,15 @@ struct AxisList {
     double w[3], f[3];
 };
 
-__device__ inline AxisList axis_list(int I, int ma) {
+__device__ inline AxisList axis_list(int I, int ma, bool p) {
     AxisList L;
     L.n = 0;
-    int last = cube_last(ma);
+    int last = cube_last(ma, p);
     for (int C = I - 1; C <= I; C++) {
-        if (C < 0 || C > last) continue;
-        bool sn = snapped(C, ma);
+        if (C < cube_first(p) || C > last) continue;
+        bool sn = snapped(C, ma, p);
         for (int d = 0; d < 2; d++) {
-            if (d && !has_upper(C, ma)) continue;
+            if (d && !has_upper(C, ma, p)) continue;
             double w = tweight(C, d, I, sn);
             if (w == 0.0) continue;
             L.C[L.n] = C; L.d[L.n] = d; L.w[L.n] = w;
@@ -46,18 +46,19 @@ static __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGe
     int I, J, K;
     decode_nat(gc, q, I, J, K);
     int s[6] = {0, 1, 0, 1, 0, 1};
-    AxisList X = axis_list(I, gf.m), Y = axis_list(J, gf.n), Z = axis_list(K, gf.o);
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    AxisList X = axis_list(I, gf.m, qx), Y = axis_list(J, gf.n, qy), Z = axis_list(K, gf.o, qz);
     for (int c = 0; c < Z.n; c++)
         for (int b = 0; b < Y.n; b++)
             for (int a = 0; a < X.n; a++) {
                 int ti = 2 * X.C[a] + X.d[a], tj = 2 * Y.C[b] + Y.d[b], tk = 2 * Z.C[c] + Z.d[c];
-                const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                const int8_t* fs = Sf + 6 * gf.pi(wrap(ti, gf.m, qx), wrap(tj, gf.n, qy), wrap(tk, gf.o, qz));
                 int lo, hi;
-                lo = fs[0] + ti; hi = fs[1] + ti; grid_map(lo, hi, gf.m);
+                lo = fs[0] + ti; hi = fs[1] + ti; grid_map(lo, hi, gf.m, qx);
                 s[0] = min(s[0], lo - I); s[1] = max(s[1], hi - I);
-                lo = fs[2] + tj; hi = fs[3] + tj; grid_map(lo, hi, gf.n);
+                lo = fs[2] + tj; hi = fs[3] + tj; grid_map(lo, hi, gf.n, qy);
                 s[2] = min(s[2], lo - J); s[3] = max(s[3], hi - J);
-                lo = fs[4] + tk; hi = fs[5] + tk; grid_map(lo, hi, gf.o);
+                lo = fs[4] + tk; hi = fs[5] + tk; grid_map(lo, hi, gf.o, qz);
                 s[4] = min(s[4], lo - K); s[5] = max(s[5], hi - K);
             }
     for (int u = 0; u < 6; u++) Sc[6 * q + u] = (int8_t)s[u];
@@ -88,44 +89,46 @@ static __global__ void __launch_bounds__(kRatBlock, 4) k_rat_fill(LevelGeom gf, 
     double acc[27];
 #pragma unroll
     for (int s = 0; s < 27; s++) acc[s] = 0.0;
-    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < 0 || cz > lz) continue;
+        if (cz < cube_first(qz) || cz > lz) continue;
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < 0 || cy > ly) continue;
+            if (cy < cube_first(qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < 0 || cx > lx) continue;
+                if (cx < cube_first(qx) || cx > lx) continue;
                 for (int dz = 0; dz < 2; dz++) {
-                    if (dz && !has_upper(cz, gf.o)) continue;
-                    bool zsn = snapped(cz, gf.o);
+                    if (dz && !has_upper(cz, gf.o, qz)) continue;
+                    bool zsn = snapped(cz, gf.o, qz);
                     if (tweight(cz, dz, K, zsn) == 0.0) continue;
                     for (int dy = 0; dy < 2; dy++) {
-                        if (dy && !has_upper(cy, gf.n)) continue;
-                        bool ysn = snapped(cy, gf.n);
+                        if (dy && !has_upper(cy, gf.n, qy)) continue;
+                        bool ysn = snapped(cy, gf.n, qy);
                         if (tweight(cy, dy, J, ysn) == 0.0) continue;
                         for (int dx = 0; dx < 2; dx++) {
-                            if (dx && !has_upper(cx, gf.m)) continue;
-                            bool xsn = snapped(cx, gf.m);
+                            if (dx && !has_upper(cx, gf.m, qx)) continue;
+                            bool xsn = snapped(cx, gf.m, qx);
                             if (tweight(cx, dx, I, xsn) == 0.0) continue;
                             double fac = ((dx && !xsn) ? 0.5 : 1.0) * ((dy && !ysn) ? 0.5 : 1.0) *
                                          ((dz && !zsn) ? 0.5 : 1.0);
                             int ti = 2 * cx + dx, tj = 2 * cy + dy, tk = 2 * cz + dz;
-                            const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                            int wi = wrap(ti, gf.m, qx), wj = wrap(tj, gf.n, qy), wk = wrap(tk, gf.o, qz);
+                            const int8_t* fs = Sf + 6 * gf.pi(wi, wj, wk);
                             int B[6] = {fs[0] + ti, fs[1] + ti, fs[2] + tj, fs[3] + tj, fs[4] + tk, fs[5] + tk};
                             int St[6] = {B[0], B[1], B[2], B[3], B[4], B[5]};
-                            grid_map(St[0], St[1], gf.m);
-                            grid_map(St[2], St[3], gf.n);
-                            grid_map(St[4], St[5], gf.o);
-                            int fcol = gf.colour(ti, tj, tk);
-                            const double* fa = Af + (long)fcol * 27 * gf.Nc + gf.cidx(ti, tj, tk);
+                            grid_map(St[0], St[1], gf.m, qx);
+                            grid_map(St[2], St[3], gf.n, qy);
+                            grid_map(St[4], St[5], gf.o, qz);
+                            int fcol = gf.colour(wi, wj, wk);
+                            const double* fa = Af + (long)fcol * 27 * gf.Nc + gf.cidx(wi, wj, wk);
 #pragma unroll
                             for (int u = 0; u < 27; u++) my[u * kRatBlock] = __ldg(fa + u * gf.Nc);
                             for (int vk = St[4]; vk < St[5]; vk++) {
-                                int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
+                                int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o, qz);
                                 for (int vj = St[2]; vj < St[3]; vj++) {
-                                    int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n);
+                                    int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n, qy);
                                     for (int vi = St[0]; vi < St[1]; vi++) {
-                                        int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m);
+                                        int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m, qx);
                                         double At = 0.0;
                                         for (int kk = lk; kk < uk; kk++) {
                                             double kfac = kk == ck ? 1.0 : 0.5;
@@ -181,44 +184,46 @@ static __global__ void __launch_bounds__(kRatSmallBlock, 4) k_rat_fill_small(Lev
     const bool mine = lane < 27;
     const int vi = I + lane % 3 - 1, vj = J + (lane / 3) % 3 - 1, vk = K + lane / 9 - 1;
     double acc = 0.0;
-    int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < 0 || cz > lz) continue;
+        if (cz < cube_first(qz) || cz > lz) continue;
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < 0 || cy > ly) continue;
+            if (cy < cube_first(qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < 0 || cx > lx) continue;
+                if (cx < cube_first(qx) || cx > lx) continue;
                 for (int dz = 0; dz < 2; dz++) {
-                    if (dz && !has_upper(cz, gf.o)) continue;
-                    bool zsn = snapped(cz, gf.o);
+                    if (dz && !has_upper(cz, gf.o, qz)) continue;
+                    bool zsn = snapped(cz, gf.o, qz);
                     if (tweight(cz, dz, K, zsn) == 0.0) continue;
                     for (int dy = 0; dy < 2; dy++) {
-                        if (dy && !has_upper(cy, gf.n)) continue;
-                        bool ysn = snapped(cy, gf.n);
+                        if (dy && !has_upper(cy, gf.n, qy)) continue;
+                        bool ysn = snapped(cy, gf.n, qy);
                         if (tweight(cy, dy, J, ysn) == 0.0) continue;
                         for (int dx = 0; dx < 2; dx++) {
-                            if (dx && !has_upper(cx, gf.m)) continue;
-                            bool xsn = snapped(cx, gf.m);
+                            if (dx && !has_upper(cx, gf.m, qx)) continue;
+                            bool xsn = snapped(cx, gf.m, qx);
                             if (tweight(cx, dx, I, xsn) == 0.0) continue;
                             double fac = ((dx && !xsn) ? 0.5 : 1.0) * ((dy && !ysn) ? 0.5 : 1.0) *
                                          ((dz && !zsn) ? 0.5 : 1.0);
                             int ti = 2 * cx + dx, tj = 2 * cy + dy, tk = 2 * cz + dz;
-                            const double* fa = Af + (long)gf.colour(ti, tj, tk) * 27 * gf.Nc + gf.cidx(ti, tj, tk);
+                            int wi = wrap(ti, gf.m, qx), wj = wrap(tj, gf.n, qy), wk = wrap(tk, gf.o, qz);
+                            const double* fa = Af + (long)gf.colour(wi, wj, wk) * 27 * gf.Nc + gf.cidx(wi, wj, wk);
                             __syncwarp();
                             if (mine) row[lane] = __ldg(fa + lane * gf.Nc);
                             __syncwarp();
-                            const int8_t* fs = Sf + 6 * gf.pi(ti, tj, tk);
+                            const int8_t* fs = Sf + 6 * gf.pi(wi, wj, wk);
                             int B[6] = {fs[0] + ti, fs[1] + ti, fs[2] + tj, fs[3] + tj, fs[4] + tk, fs[5] + tk};
                             int St[6] = {B[0], B[1], B[2], B[3], B[4], B[5]};
-                            grid_map(St[0], St[1], gf.m);
-                            grid_map(St[2], St[3], gf.n);
-                            grid_map(St[4], St[5], gf.o);
+                            grid_map(St[0], St[1], gf.m, qx);
+                            grid_map(St[2], St[3], gf.n, qy);
+                            grid_map(St[4], St[5], gf.o, qz);
                             if (!mine || vi < St[0] || vi >= St[1] || vj < St[2] || vj >= St[3] || vk < St[4] ||
                                 vk >= St[5])
                                 continue;
-                            int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
-                            int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n);
-                            int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m);
+                            int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o, qz);
+                            int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n, qy);
+                            int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m, qx);
                             double At = 0.0;
                             for (int kk = lk; kk < uk; kk++) {
                                 double kfac = kk == ck ? 1.0 : 0.5;
@@ -245,16 +250,28 @@ static __global__ void __launch_bounds__(kRatSmallBlock, 4) k_rat_fill_small(Lev
 // ---------------------------------------------------------------------------
 // Coarsest level: dense column-major matrix Aexact[row + col*n] from the
 // level's stencils (region_tr.cc:489-508, non-periodic: no wrap needed).
-static __global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, double* __restrict__ M) {
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+static __global__ void k_lu_build(LevelGeom g, const double* __restrict__ A, const int8_t* __restrict__ S,
+                                  double* __restrict__ M) {
+    // One thread per row, the box's entries in box order (dk, dj, di
+    // ascending), column indices wrapped on periodic axes (step_mod,
+    // region.hh:466); an entry is assigned, so when two entries of a row wrap
+    // onto one column (a periodic axis of size 1 or 2) the later one stays,
+    // as in the reference.
+    long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long n = g.npts;
-    if (q >= n * 27) return;
-    long row = q / 27;
-    int s = (int)(q % 27);
+    if (row >= n) return;
     int i = (int)(row % g.m); long t = row / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
-    int ii = i + s % 3 - 1, jj = j + (s / 3) % 3 - 1, kk = k + s / 9 - 1;
-    if (ii < 0 || jj < 0 || kk < 0 || ii >= g.m || jj >= g.n || kk >= g.o) return;
-    M[row + g.pi(ii, jj, kk) * n] = A[g.ai(i, j, k, s)];
+    const int8_t* b = S + 6 * row;
+    for (int dk = b[4]; dk < b[5]; dk++)
+        for (int dj = b[2]; dj < b[3]; dj++)
+            for (int di = b[0]; di < b[1]; di++) {
+                int ii = i + di, jj = j + dj, kk = k + dk;
+                ii = ii < 0 ? ii + g.m : (ii >= g.m ? ii - g.m : ii);
+                jj = jj < 0 ? jj + g.n : (jj >= g.n ? jj - g.n : jj);
+                kk = kk < 0 ? kk + g.o : (kk >= g.o ? kk - g.o : kk);
+                int s = (di + 1) + 3 * (dj + 1) + 9 * (dk + 1);
+                M[row + g.pi(ii, jj, kk) * n] = A[g.ai(i, j, k, s)];
+            }
 }
 
 // Explicit inverse from the factors: column c of Minv (row-major) solves

@@ -30,6 +30,7 @@ struct LevelGeom {
     long mx, my;     // halo'd x strides: m+2, n+2
     long xsize;      // (m+2)(n+2)(o+2)
     long npts;       // m*n*o
+    int prd;         // periodic axes: bit 0 x, bit 1 y, bit 2 z
 
     __host__ __device__ inline long xi(int i, int j, int k) const {
         return (i + 1) + mx * ((j + 1) + my * (long)(k + 1));
@@ -71,9 +72,10 @@ __host__ __device__ __forceinline__ void decode_nat(const LevelGeom& g, long q, 
     j = (int)(t - (unsigned)k * n);
 }
 
-inline LevelGeom make_geom(int m, int n, int o) {
+inline LevelGeom make_geom(int m, int n, int o, int prd = 0) {
     LevelGeom g;
     g.m = m; g.n = n; g.o = o;
+    g.prd = prd;
     g.M2 = (m + 1) / 2; g.N2 = (n + 1) / 2; g.O2 = (o + 1) / 2;
     long nc = (long)g.M2 * g.N2 * g.O2;
     g.Nc = (nc + 63) / 64 * 64;
@@ -106,9 +108,25 @@ __host__ __device__ inline int slab_lo(const LevelGeom& g, int s, int slabs) {
 // exists; the upper point 2C+1 exists unless C is the last cube of an odd
 // axis; on an even axis the last cube's upper point (ma-1) "snaps" onto
 // coarse C+1 with weight 1 (mask bits 4/32/256).
-__host__ __device__ inline int cube_last(int ma) { int sm = (ma + 2) >> 1; return (ma & 1) ? sm - 1 : sm - 2; }
-__host__ __device__ inline bool has_upper(int C, int ma) { return 2 * C + 1 < ma; }
-__host__ __device__ inline bool snapped(int C, int ma) { return !(ma & 1) && C == cube_last(ma); }
+// A periodic axis (p; even ma, coarse size ma/2, region.cc:14) has cubes
+// C = -1..ma/2-1, all with both points and none snapped: cube -1 is the image
+// of cube ma/2-1, whose upper point ma-1 sits just below fine point 0 and
+// also transfers to coarse 0.  Indices of such images are unwrapped here and
+// wrapped only to address memory (wrap()).
+__host__ __device__ inline int cube_first(bool p) { return p ? -1 : 0; }
+__host__ __device__ inline int cube_last(int ma, bool p = false) {
+    if (p) return (ma >> 1) - 1;
+    int sm = (ma + 2) >> 1;
+    return (ma & 1) ? sm - 1 : sm - 2;
+}
+__host__ __device__ inline bool has_upper(int C, int ma, bool p = false) { return p || 2 * C + 1 < ma; }
+__host__ __device__ inline bool snapped(int C, int ma, bool p = false) { return !p && !(ma & 1) && C == cube_last(ma); }
+__host__ __device__ inline int wrap(int v, int size, bool p) {
+    return p ? (v < 0 ? v + size : (v >= size ? v - size : v)) : v;
+}
+__host__ __device__ inline bool px(const LevelGeom& g) { return g.prd & 1; }
+__host__ __device__ inline bool py(const LevelGeom& g) { return (g.prd >> 1) & 1; }
+__host__ __device__ inline bool pz(const LevelGeom& g) { return (g.prd >> 2) & 1; }
 
 // Weight of fine role d (0 lower, 1 upper) of cube C onto coarse index I,
 // 0 if the fine point does not transfer to I.
@@ -118,21 +136,45 @@ __host__ __device__ inline double tweight(int C, int d, int I, bool snap) {
     return (C == I || C + 1 == I) ? 0.5 : 0.0;
 }
 
-// grid_map, non-periodic (region.cc:1209-1216).
-__host__ __device__ inline void grid_map(int& lo, int& hi, int ma) {
+// grid_map (region.cc:1201-1217): a fine global box bound to the coarse one.
+__host__ __device__ inline void grid_map(int& lo, int& hi, int ma, bool p = false) {
+    if (p) {
+        lo = lo < 0 ? (lo - ((ma & 1) ? 2 : 1)) / 2 : lo >> 1;
+        hi = (hi + (((ma & 1) && hi > ma) ? 3 : 2)) >> 1;
+        return;
+    }
     lo = (!(ma & 1) && lo == ma - 1 ? lo + 1 : lo) >> 1;
     hi = (hi + 2) >> 1;
 }
 
-// igrid_map, non-periodic, with the crop to the stencil box (region.cc:1243-1258).
-__host__ __device__ inline int igrid_map(int& lo, int& hi, int blo, int bhi, int i, int ma) {
+// igrid_map with the crop to the stencil box (region.cc:1231-1259): the fine
+// range a coarse index gathers from, and its coincident fine index.  Periodic
+// axes here are even (coarse index i <-> fine 2i, range [2i-1, 2i+2)).
+__host__ __device__ inline int igrid_map(int& lo, int& hi, int blo, int bhi, int i, int ma, bool p = false) {
     int j = i << 1;
-    if (ma & 1) { lo = j == 0 ? 0 : j - 1; hi = j == ma - 1 ? ma : j + 2; }
+    if (p) { lo = j - 1; hi = j + 2; }
+    else if (ma & 1) { lo = j == 0 ? 0 : j - 1; hi = j == ma - 1 ? ma : j + 2; }
     else if (j == ma) { lo = ma - 1; hi = ma; j = ma - 1; }
     else { lo = j == 0 ? 0 : j - 1; hi = j == ma - 2 ? ma - 1 : j + 2; }
     if (lo < blo) lo = blo;
     if (hi > bhi) hi = bhi;
     return j;
+}
+
+// Periodic images in the one-point halo of x: halo index -1 holds the value
+// of size-1 and halo index size that of 0, on periodic axes only (the halo of
+// a non-periodic axis stays zero).  Writes v at (i,j,k)'s images.
+template <class T>
+__device__ __forceinline__ void store_images(const LevelGeom& g, T* x, int i, int j, int k, T v) {
+    int ia = (g.prd & 1) ? (i == 0 ? g.m : (i == g.m - 1 ? -1 : -2)) : -2;
+    int ja = (g.prd & 2) ? (j == 0 ? g.n : (j == g.n - 1 ? -1 : -2)) : -2;
+    int ka = (g.prd & 4) ? (k == 0 ? g.o : (k == g.o - 1 ? -1 : -2)) : -2;
+    if (ia == -2 && ja == -2 && ka == -2) return;
+    for (int s = 1; s < 8; s++) {
+        int ii = (s & 1) ? ia : i, jj = (s & 2) ? ja : j, kk = (s & 4) ? ka : k;
+        if (ii == -2 || jj == -2 || kk == -2) continue;
+        x[g.xi(ii, jj, kk)] = v;
+    }
 }
 
 // Arithmetic helpers: EXACT = round every product and sum separately, as the

@@ -38,3 +38,31 @@ def relerr(a, b):
     b = np.asarray(b, float)
     den = np.abs(b).max()
     return np.abs(a - b).max() / (den if den > 0 else 1.0)
+
+
+def periodic_problem(m, n, o, prd, seed=0, shift=0.3, spread=0.2):
+    """Random 27-point stencils on an m x n x o grid with the axes flagged in
+    prd periodic: a 27-point Q1-Laplacian pattern (centre 8/3 + shift, edge
+    -1/6, corner -1/12, face 0) with every entry scaled by 1 + U(-spread,
+    spread); full [-1,2) boxes on periodic axes, boxes cropped at the
+    boundary of non-periodic ones.  Returns (coef27, S6, r)."""
+    rng = np.random.default_rng(seed)
+    N = m * n * o
+    slots = np.arange(27)
+    d = np.stack([slots % 3 - 1, (slots // 3) % 3 - 1, slots // 9 - 1], 1)
+    nd = np.abs(d).sum(1)
+    base = np.select([nd == 0, nd == 1, nd == 2, nd == 3], [8.0 / 3.0 + shift, 0.0, -1.0 / 6.0, -1.0 / 12.0])
+    k, j, i = np.meshgrid(np.arange(o), np.arange(n), np.arange(m), indexing="ij")
+    idx = [i.reshape(-1), j.reshape(-1), k.reshape(-1)]
+    size = [m, n, o]
+    S = np.zeros((N, 6), np.int32)
+    ok = np.ones((N, 27), bool)
+    for a in range(3):
+        lo = np.where(prd[a] | (idx[a] > 0), -1, 0)
+        hi = np.where(prd[a] | (idx[a] < size[a] - 1), 2, 1)
+        S[:, 2 * a], S[:, 2 * a + 1] = lo, hi
+        ok &= (d[None, :, a] >= lo[:, None]) & (d[None, :, a] < hi[:, None])
+    coef = base[None, :] * (1.0 + spread * rng.uniform(-1, 1, (N, 27)))
+    coef[~ok] = 0.0
+    r = rng.uniform(-1, 1, N)
+    return coef, S, r

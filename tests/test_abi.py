@@ -78,8 +78,12 @@ def test_create_rejects_bad_args():
     d = P.Dims(1, 9, 9, 0, 0, 0, 0, 0, 0, -1)
     h = C.c_void_p()
     assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 7
-    d = P.Dims(9, 9, 9, 1, 0, 0, 0, 0, 0, -1)
-    assert P.lib().pgmg_dev_create(C.byref(d), C.byref(h)) == 11
+    # Periodic axes pass argument checks (without a GPU: no device).
+    d = P.Dims(8, 9, 9, 1, 0, 0, 0, 0, 0, -1)
+    rc = P.lib().pgmg_dev_create(C.byref(d), C.byref(h))
+    assert rc in (0, 12)
+    if rc == 0:
+        P.lib().pgmg_dev_destroy(h)
 
 
 def test_q1_variable_kappa_stencil_symmetric():
