@@ -71,13 +71,13 @@ void carve(pgmg_handle* h) {
         Level& L = h->L[l];
         const LevelGeom& g = L.g;
         L.A64 = a.take<double>(8 * 27 * g.Nc);
-        L.x64 = a.take<double>(g.xsize);
+        L.x64 = a.take<double>(g.xsize());
         L.r64 = a.take<double>(8 * g.Nc);
         L.res64 = a.take<double>(8 * g.Nc);
         L.S = a.take<int8_t>(6 * g.npts);
         if (mixed) {
             L.A32 = a.take<float>(8 * 27 * g.Nc);
-            L.x32 = a.take<float>(g.xsize);
+            L.x32 = a.take<float>(g.xsize());
             L.r32 = a.take<float>(8 * g.Nc);
             L.res32 = a.take<float>(8 * g.Nc);
         }
@@ -139,14 +139,15 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
     if (g.prd && ((px(g) && (g.m & 1)) || (py(g) && (g.n & 1)) || (pz(g) && (g.o & 1))))
         smoother = PGMG_SMOOTH_LEX;
     if (smoother == PGMG_SMOOTH_LEX && g.prd) {
-        // region::gauss_seidel (region.cc:355-361) refreshes the ghosts once
-        // per call and sweeps with them fixed: the images are refreshed
-        // before each sweep (and after the last), and the hyperplane kernel
-        // reads but never writes them.
+        // region::gauss_seidel (region.cc:355-361, 456-457) refreshes the
+        // ghosts before the forward and before the backward pass and sweeps
+        // with them fixed: the images are refreshed before each pass (and
+        // after the last), and the hyperplane kernel reads but never writes
+        // them.
         int np = num_planes(g);
         for (int s = 0; s < sweeps; s++) {
-            TRY(wrap_level<T>(h, l));
-            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++) {
+                TRY(wrap_level<T>(h, l));
                 for (int tt = 0; tt < np; tt++) {
                     int t = pass ? np - 1 - tt : tt;
                     Plane P = plane_range(g, t);
@@ -154,6 +155,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                     if (nw <= 0) continue;
                     LAUNCH(nblk(nw), kBlock, k_gs_plane<T>, g, v.x, v.r, v.A, t, P);
                 }
+            }
         }
         return wrap_level<T>(h, l);
     }
@@ -187,7 +189,10 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 long np = (long)(k2hi - k2lo) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
                     int col = pass ? 7 - cc : cc;
-                    LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
+                    if (g.prd)
+                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
+                    else
+                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
                 }
             }
     return PGMG_OK;
@@ -209,7 +214,10 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     Level& Cl = h->L[l];
     View<T> vf = view<T>(F), vc = view<T>(Cl);
     TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
-    LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
+    if (F.g.prd)
+        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T, true>, F.g, Cl.g, vf.res, vc.r, vc.x);
+    else
+        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
     return wrap_level<T>(h, l);
 }
 

@@ -36,7 +36,7 @@ __device__ __forceinline__ T gs_value(const LevelGeom& g, const T* __restrict__ 
 // consecutive threads is contiguous (structure-of-arrays per colour).
 // One colour point p (index inside colour `col`): the body of k_gs_colour,
 // shared with the batched kernels.
-template <class T>
+template <class T, bool PRD = false>
 __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* __restrict__ r,
                                              const T* __restrict__ A, int col, long p) {
     int i2, j2, k2;
@@ -48,18 +48,20 @@ __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* 
     const T* Ap = A + (long)col * 27 * g.Nc + p;
     T v = gs_value<T, true>(g, x, xc, Ap, g.Nc, ld_stream(r + (long)col * g.Nc + p, ps), ps, pk);
     st_keep(x + xc, v, pk);
-    // Periodic axes: the point's images in the halo are updated with it; the
-    // points that read them are of other colours (periodic sizes are even).
-    if (g.prd) store_images<T>(g, x, i, j, k, v);
+    // Periodic axes (PRD: a separate instantiation, so that the usual one
+    // keeps its register count): the point's images in the halo are updated
+    // with it; the points that read them are of other colours (periodic sizes
+    // are even).
+    if (PRD) store_images<T>(g, x, i, j, k, v);
 }
 
-template <class T, bool EXACT>
+template <class T, bool EXACT, bool PRD = false>
 __global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
                                                       const T* __restrict__ A, int col, int k2lo, int k2hi) {
     pdl_enter();
     long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (p >= (long)k2hi * g.M2 * g.N2) return;
-    gs_colour_at<T>(g, x, r, A, col, p);
+    gs_colour_at<T, PRD>(g, x, r, A, col, p);
 }
 
 // Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of
@@ -312,13 +314,14 @@ static __global__ void __launch_bounds__(1024) k_reduce_partials(const double* _
 // reference's restrict_partial tests the x snap flag for the y axis of the
 // (ti,tj+1,tk+1) point (region.cc:888-895); that is kept, see ysnap below.
 // Also clears the coarse x (multigrid.cc:219).
-template <class T>
+template <class T, bool PRD = false>
 __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
                                             T* __restrict__ rc, T* __restrict__ xc, long q) {
     if (q >= gc.npts) return;
     int I, J, K;
     decode_nat(gc, q, I, J, K);
-    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    // PRD: the instantiation for levels with periodic axes.
+    const bool qx = PRD && px(gf), qy = PRD && py(gf), qz = PRD && pz(gf);
     int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     T acc = T(0);
     for (int cz = K - 1; cz <= K; cz++) {
@@ -354,11 +357,11 @@ __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom
     xc[gc.xi(I, J, K)] = T(0);
 }
 
-template <class T>
+template <class T, bool PRD = false>
 __global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
                                                      T* __restrict__ rc, T* __restrict__ xc) {
     pdl_enter();
-    restrict_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
+    restrict_at<T, PRD>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
 // Interpolation with correction add (region.cc:576-593): each fine point

@@ -28,10 +28,11 @@ struct LevelGeom {
     int M2, N2, O2;  // colour sub-grid size, (m+1)/2 ...
     long Nc;         // padded points per colour
     long mx, my;     // halo'd x strides: m+2, n+2
-    long xsize;      // (m+2)(n+2)(o+2)
-    long npts;       // m*n*o
     int prd;         // periodic axes: bit 0 x, bit 1 y, bit 2 z
+    int pad_;
+    long npts;       // m*n*o
 
+    __host__ __device__ inline long xsize() const { return mx * my * (long)(o + 2); }  // halo'd x
     __host__ __device__ inline long xi(int i, int j, int k) const {
         return (i + 1) + mx * ((j + 1) + my * (long)(k + 1));
     }
@@ -80,7 +81,7 @@ inline LevelGeom make_geom(int m, int n, int o, int prd = 0) {
     long nc = (long)g.M2 * g.N2 * g.O2;
     g.Nc = (nc + 63) / 64 * 64;
     g.mx = m + 2; g.my = n + 2;
-    g.xsize = (long)(m + 2) * (n + 2) * (o + 2);
+    g.pad_ = 0;
     g.npts = (long)m * n * o;
     return g;
 }
@@ -93,7 +94,7 @@ inline LevelGeom make_geom(int m, int n, int o, int prd = 0) {
 // on the level size, the element size and the budget, so the oracle can
 // reproduce the same order.
 __host__ __device__ inline int slab_count(const LevelGeom& g, int elem_bytes, long long budget) {
-    long long bytes = (long long)g.xsize * elem_bytes;
+    long long bytes = (long long)g.xsize() * elem_bytes;
     if (budget <= 0 || bytes <= budget) return 1;
     long long s = (bytes + budget - 1) / budget;
     return (int)(s < g.O2 ? s : g.O2);
