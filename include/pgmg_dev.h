@@ -55,7 +55,8 @@ typedef enum {
     PGMG_ERR_CUDA = 8,         /* a CUDA runtime call failed                */
     PGMG_ERR_TIMEOUT = 9,      /* a bounded device wait ran out             */
     PGMG_ERR_ADMISSION = 10,   /* request does not fit the memory cap       */
-    PGMG_ERR_UNSUPPORTED = 11, /* feature not built (e.g. periodic axes)    */
+    PGMG_ERR_UNSUPPORTED = 11, /* configuration not supported (e.g. a periodic
+                                  axis odd on a level above the coarsest) */
     PGMG_ERR_NO_DEVICE = 12    /* no CUDA device visible                    */
 } pgmg_status;
 
@@ -95,7 +96,9 @@ typedef struct pgmg_handle pgmg_handle;
  * (geometry.cc:12-26) on one process, plus the run-time choices. */
 typedef struct {
     int m, n, o;              /* global grid size                          */
-    int x_prd, y_prd, z_prd;  /* periodicity (non-zero: periodic)          */
+    int x_prd, y_prd, z_prd;  /* periodicity (non-zero: periodic; the axis
+                                 must be even on every level but the
+                                 coarsest; coarse size (m+1)>>1, region.cc:14) */
     int precision;            /* PGMG_FP64 or PGMG_MIXED                    */
     int coarse;               /* PGMG_COARSE_LU or PGMG_COARSE_GS           */
     int smoother;             /* default smoother of pgmg_dev_vcycle        */
