@@ -145,7 +145,10 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *   PGMG_OPT_PDL            1 = launch the V-cycle's kernels as programmatic
  *                           dependent launches, so that each is scheduled while
  *                           the one before it drains (default); 0 = plain
- *                           launches.  No counterpart in the reference. */
+ *                           launches.  No counterpart in the reference.
+ *   PGMG_OPT_GS_BLOCK       threads per block of the 8-colour sweep kernel:
+ *                           128, 256 (default) or 512.  No counterpart in the
+ *                           reference. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -154,9 +157,20 @@ enum {
     PGMG_OPT_V_DOWN = 5,
     PGMG_OPT_V_UP = 6,
     PGMG_OPT_V_BOTTOM = 7,
-    PGMG_OPT_PDL = 8
+    PGMG_OPT_PDL = 8,
+    PGMG_OPT_GS_BLOCK = 9
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
+/* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
+ * one untimed) of this handle's problem under candidate values of the
+ * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
+ * PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_PDL -- one option at a time from the best so
+ * far, and keeps the fastest.  The level-0 solution is saved and restored.
+ * The choice is remembered for the process per (grid, periodic axes,
+ * precision, smoother, device): a later handle of the same shape takes it
+ * without timing.  *ms (may be NULL): the chosen V-cycle time.  Needs
+ * pgmg_dev_build_rat; synchronises. */
+pgmg_status pgmg_dev_autotune(pgmg_handle *h, int reps, double *ms);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
 /* Default smoother of pgmg_dev_vcycle and the solves. */
 pgmg_status pgmg_dev_set_smoother(pgmg_handle *h, int smoother);

@@ -28,6 +28,7 @@ FIELD_X, FIELD_R, FIELD_RES = 0, 1, 2
 OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE, OPT_SLAB_BUDGET = 1, 2, 3, 4
 OPT_V_DOWN, OPT_V_UP, OPT_V_BOTTOM = 5, 6, 7
 OPT_PDL = 8
+OPT_GS_BLOCK = 9
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -68,6 +69,7 @@ SIGNATURES = [
     ("pgmg_dev_set_smoother", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_set_option", C.c_int, [_VP, C.c_int, C.c_longlong]),
     ("pgmg_dev_get_option", C.c_int, [_VP, C.c_int, C.POINTER(C.c_longlong)]),
+    ("pgmg_dev_autotune", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
     ("pgmg_dev_num_levels", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("pgmg_dev_level_dims", C.c_int, [_VP, C.c_int, _ip]),
     ("pgmg_dev_memory", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
@@ -263,6 +265,16 @@ class Multigrid:
         v = C.c_longlong()
         self._ck(lib().pgmg_dev_get_option(self._h, key, C.byref(v)), "get_option")
         return v.value
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Times V-cycles under the result-neutral execution options and keeps
+        the fastest (pgmg_dev_autotune); returns the chosen options and the
+        V-cycle time in ms."""
+        ms = C.c_double()
+        self._ck(lib().pgmg_dev_autotune(self._h, int(reps), C.byref(ms)), "autotune")
+        return {"gs_block": self.get_option(OPT_GS_BLOCK), "cluster_first": self.get_option(OPT_CLUSTER_FIRST),
+                "cluster_size": self.get_option(OPT_CLUSTER_SIZE), "pdl": self.get_option(OPT_PDL),
+                "vcycle_ms": ms.value}
 
     def set_smoother(self, smoother: int):
         self._ck(lib().pgmg_dev_set_smoother(self._h, smoother), "set_smoother")

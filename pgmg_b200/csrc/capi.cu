@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -191,6 +192,12 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                     int col = pass ? 7 - cc : cc;
                     if (g.prd)
                         LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
+                    else if (h->gs_block == 128)
+                        LAUNCH(nblk(np, 128), 128, k_gs_colour<T, true, false, 128>, g, v.x, v.r, v.A, col, k2lo,
+                               k2hi);
+                    else if (h->gs_block == 512)
+                        LAUNCH(nblk(np, 512), 512, k_gs_colour<T, true, false, 512>, g, v.x, v.r, v.A, col, k2lo,
+                               k2hi);
                     else
                         LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
                 }
@@ -650,6 +657,11 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_PDL:
             h->pdl = value != 0;
             break;
+        case PGMG_OPT_GS_BLOCK:
+            if (value != 128 && value != 256 && value != 512)
+                return fail(h, PGMG_ERR_ARG, "colour-sweep block must be 128, 256 or 512 threads");
+            h->gs_block = (int)value;
+            break;
         case PGMG_OPT_V_DOWN:
         case PGMG_OPT_V_UP:
         case PGMG_OPT_V_BOTTOM:
@@ -675,6 +687,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_V_UP: *value = h->v_up; return PGMG_OK;
         case PGMG_OPT_V_BOTTOM: *value = h->v_bottom; return PGMG_OK;
         case PGMG_OPT_PDL: *value = h->pdl; return PGMG_OK;
+        case PGMG_OPT_GS_BLOCK: *value = h->gs_block; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -951,6 +964,137 @@ pgmg_status pgmg_dev_vcycle(pgmg_handle* h, int mode, int smoother) {
     h->x0_zero = false;
     if (h->dims.precision == PGMG_MIXED) return ir_step(h, mode, smoother, nullptr, nullptr);
     return run_vcycle<double>(h, mode, smoother);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Autotuner state: the options chosen for a problem shape, remembered for
+// the process.
+struct TuneKey {
+    int m, n, o, prd, precision, smoother, device;
+    bool operator==(const TuneKey& b) const {
+        return m == b.m && n == b.n && o == b.o && prd == b.prd && precision == b.precision &&
+               smoother == b.smoother && device == b.device;
+    }
+};
+struct TuneVal {
+    int gs_block, coarse_first, cluster_size, pdl;
+    double ms;
+};
+std::mutex g_tune_mu;
+std::vector<std::pair<TuneKey, TuneVal>> g_tune;
+
+void apply_tuning(pgmg_handle* h, const TuneVal& v) {
+    h->gs_block = v.gs_block;
+    h->coarse_first = v.coarse_first;
+    h->cluster_size = v.cluster_size;
+    h->pdl = v.pdl != 0;
+    drop_graphs(h);
+}
+
+// Mean time of `reps` V-cycles (after one untimed cycle, which also captures
+// the graph) under the handle's current options.
+pgmg_status time_vcycles(pgmg_handle* h, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+    drop_graphs(h);
+    TRY(upload_plans(h));
+    TRY(pgmg_dev_vcycle(h, 0, -1));
+    CK(cudaEventRecord(e0, h->stream));
+    for (int i = 0; i < reps; i++) TRY(pgmg_dev_vcycle(h, 0, -1));
+    CK(cudaEventRecord(e1, h->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / reps;
+    return PGMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
+    if (!h) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (reps < 1) reps = 3;
+    TuneKey key{h->dims.m, h->dims.n, h->dims.o, h->prd, h->dims.precision, h->dims.smoother, h->device};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (auto& kv : g_tune)
+            if (kv.first == key) {
+                apply_tuning(h, kv.second);
+                TRY(upload_plans(h));
+                if (best_ms) *best_ms = kv.second.ms;
+                return PGMG_OK;
+            }
+    }
+    // Save the level-0 solution (and whether it is known to be zero); the
+    // timed V-cycles change it.
+    Level& L0 = h->L[0];
+    const LevelGeom& g0 = L0.g;
+    bool zero = h->x0_zero;
+    k_x_to_nat<double><<<nblk(g0.npts), kBlock, 0, h->stream>>>(g0, L0.x64, h->stage);
+    CKL();
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, 0};
+    pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
+    auto trial = [&](TuneVal c) -> pgmg_status {
+        apply_tuning(h, c);
+        double t = 0;
+        pgmg_status s2 = time_vcycles(h, reps, e0, e1, &t);
+        if (s2 != PGMG_OK) return s2;
+        c.ms = t;
+        if (t < best.ms) best = c;
+        return PGMG_OK;
+    };
+    bool mc8 = h->dims.smoother == PGMG_SMOOTH_MC8;
+    // Coordinate descent: one option at a time, each from the best so far.
+    if (st == PGMG_OK && mc8 && !h->prd)
+        for (int b : {128, 512}) {
+            TuneVal c = best;
+            c.gs_block = b;
+            if ((st = trial(c)) != PGMG_OK) break;
+        }
+    if (st == PGMG_OK && mc8 && h->cluster_size > 0 && h->dims.coarse != PGMG_COARSE_LU_EXACT) {
+        int f0 = best.coarse_first;
+        for (int l = 0; l <= h->nl && st == PGMG_OK; l++) {
+            if (l == f0 || (l < h->nl && h->L[l].g.npts > 6 * kClusterMax)) continue;
+            TuneVal c = best;
+            c.coarse_first = l;
+            st = trial(c);
+        }
+        int other = best.cluster_size == 16 ? 8 : 16;
+        if (st == PGMG_OK && probe_cluster<double>(other) > 0 && probe_cluster<float>(other) > 0) {
+            TuneVal c = best;
+            c.cluster_size = other;
+            st = trial(c);
+        }
+    }
+    if (st == PGMG_OK) {
+        TuneVal c = best;
+        c.pdl = !best.pdl;
+        st = trial(c);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    apply_tuning(h, best);
+    TRY(upload_plans(h));
+    // Restore the solution.
+    k_nat_to_x<double><<<nblk(g0.npts), kBlock, 0, h->stream>>>(g0, h->stage, L0.x64);
+    CKL();
+    TRY(wrap_level<double>(h, 0));
+    CK(cudaStreamSynchronize(h->stream));
+    h->x0_zero = zero;
+    if (st != PGMG_OK) return st;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune.push_back({key, best});
+    }
+    if (best_ms) *best_ms = best.ms;
+    return PGMG_OK;
 }
 
 pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {

@@ -97,7 +97,8 @@ struct pgmg_handle {
     long long vgraph_nodes[2][2][2] = {};
     bool use_graphs = true;
     int prd = 0;      // periodic axes of the problem (bit 0 x, 1 y, 2 z)
-    bool pdl = true;  // V-cycle and solve-loop kernels as programmatic dependent launches
+    bool pdl = true;
+    int gs_block = 256;  // threads per block of the colour sweep  // V-cycle and solve-loop kernels as programmatic dependent launches
     // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
     // first level it handles.
     int cluster_size = 0;

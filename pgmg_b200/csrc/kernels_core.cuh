@@ -55,8 +55,9 @@ __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* 
     if (PRD) store_images<T>(g, x, i, j, k, v);
 }
 
-template <class T, bool EXACT, bool PRD = false>
-__global__ void __launch_bounds__(kBlock) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
+// BS: threads per block (the autotuner picks 128, 256 or 512 per handle).
+template <class T, bool EXACT, bool PRD = false, int BS = kBlock>
+__global__ void __launch_bounds__(BS) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
                                                       const T* __restrict__ A, int col, int k2lo, int k2hi) {
     pdl_enter();
     long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;

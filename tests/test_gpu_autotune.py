@@ -1,0 +1,51 @@
+"""The autotuner (pgmg_dev_autotune) and the options it chooses among: every
+candidate must leave the iterates bit for bit unchanged, the chosen options
+must be valid, and a second handle of the same shape takes the remembered
+choice."""
+import numpy as np
+import pytest
+
+import pgmg_b200 as P
+from tests.helpers import q1_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def make(mno, precision):
+    coef, S, r = q1_problem(*mno, sigma=1.0, seed=sum(mno))
+    G = P.Multigrid(*mno, precision=precision)
+    G.setup_matrices(coef, S)
+    G.setup_fields(r)
+    return G
+
+
+@pytest.mark.parametrize("mno", [(65, 65, 65), (33, 40, 17)])
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_autotune_changes_no_result(mno, precision):
+    A = make(mno, precision)
+    A.solve(1e-10, 100, 1)
+    xa = A.get_x(0)
+    B = make(mno, precision)
+    t = B.autotune()
+    assert t["gs_block"] in (128, 256, 512) and t["pdl"] in (0, 1) and t["vcycle_ms"] > 0
+    assert 0 <= t["cluster_first"] <= B.nlevels and t["cluster_size"] in (8, 16)
+    B.clear_x(0)
+    B.solve(1e-10, 100, 1)
+    assert np.array_equal(B.get_x(0), xa)
+    # The same shape again: the remembered choice, without timing.
+    C = make(mno, precision)
+    t2 = C.autotune()
+    assert {k: t2[k] for k in ("gs_block", "cluster_first", "cluster_size", "pdl")} == \
+           {k: t[k] for k in ("gs_block", "cluster_first", "cluster_size", "pdl")}
+
+
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_gs_block_bitwise(block):
+    mno = (41, 41, 41)
+    A = make(mno, P.FP64)
+    B = make(mno, P.FP64)
+    B.set_option(P.OPT_GS_BLOCK, block)
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
