@@ -148,7 +148,14 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           launches.  No counterpart in the reference.
  *   PGMG_OPT_GS_BLOCK       threads per block of the 8-colour sweep kernel:
  *                           128, 256 (default) or 512.  No counterpart in the
- *                           reference. */
+ *                           reference.
+ *   PGMG_OPT_GRID_MAX       8-colour levels of at most this many points (and
+ *                           above the cluster levels) sweep each V-cycle leg in
+ *                           one persistent whole-GPU launch whose colour passes
+ *                           are separated by a grid barrier with a bounded wait
+ *                           (a wait that runs out makes the solve return
+ *                           PGMG_ERR_TIMEOUT); 0 = off (default).  No
+ *                           counterpart in the reference. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -158,19 +165,26 @@ enum {
     PGMG_OPT_V_UP = 6,
     PGMG_OPT_V_BOTTOM = 7,
     PGMG_OPT_PDL = 8,
-    PGMG_OPT_GS_BLOCK = 9
+    PGMG_OPT_GS_BLOCK = 9,
+    PGMG_OPT_GRID_MAX = 10
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
- * PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_PDL -- one option at a time from the best so
+ * PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_GRID_MAX, PGMG_OPT_PDL -- one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,
  * precision, smoother, device): a later handle of the same shape takes it
  * without timing.  *ms (may be NULL): the chosen V-cycle time.  Needs
  * pgmg_dev_build_rat; synchronises. */
 pgmg_status pgmg_dev_autotune(pgmg_handle *h, int reps, double *ms);
+/* Self-check of the persistent sweep kernel's bounded grid barrier (no
+ * counterpart in the reference): one FP64 8-colour sweep of `level` in one
+ * cooperative launch; with run_out != 0 the barrier waits for one block more
+ * than the launch has, so its wait runs out (about a second) and the call
+ * returns PGMG_ERR_TIMEOUT with the device usable; otherwise PGMG_OK. */
+pgmg_status pgmg_dev_grid_check(pgmg_handle *h, int level, int run_out);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
 /* Default smoother of pgmg_dev_vcycle and the solves. */
 pgmg_status pgmg_dev_set_smoother(pgmg_handle *h, int smoother);

@@ -29,6 +29,7 @@ OPT_GRAPHS, OPT_CLUSTER_FIRST, OPT_CLUSTER_SIZE, OPT_SLAB_BUDGET = 1, 2, 3, 4
 OPT_V_DOWN, OPT_V_UP, OPT_V_BOTTOM = 5, 6, 7
 OPT_PDL = 8
 OPT_GS_BLOCK = 9
+OPT_GRID_MAX = 10
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -70,6 +71,7 @@ SIGNATURES = [
     ("pgmg_dev_set_option", C.c_int, [_VP, C.c_int, C.c_longlong]),
     ("pgmg_dev_get_option", C.c_int, [_VP, C.c_int, C.POINTER(C.c_longlong)]),
     ("pgmg_dev_autotune", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
+    ("pgmg_dev_grid_check", C.c_int, [_VP, C.c_int, C.c_int]),
     ("pgmg_dev_num_levels", C.c_int, [_VP, C.POINTER(C.c_int)]),
     ("pgmg_dev_level_dims", C.c_int, [_VP, C.c_int, _ip]),
     ("pgmg_dev_memory", C.c_int, [_VP, C.POINTER(C.c_size_t)]),
@@ -274,6 +276,7 @@ class Multigrid:
         self._ck(lib().pgmg_dev_autotune(self._h, int(reps), C.byref(ms)), "autotune")
         return {"gs_block": self.get_option(OPT_GS_BLOCK), "cluster_first": self.get_option(OPT_CLUSTER_FIRST),
                 "cluster_size": self.get_option(OPT_CLUSTER_SIZE), "pdl": self.get_option(OPT_PDL),
+                "grid_max": self.get_option(OPT_GRID_MAX),
                 "vcycle_ms": ms.value}
 
     def set_smoother(self, smoother: int):

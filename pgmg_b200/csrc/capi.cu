@@ -94,6 +94,7 @@ void carve(pgmg_handle* h) {
         h->piv = a.take<int>(n);
     }
     h->info = a.take<int>(4);
+    h->bar = a.take<GridBar>(1);
     h->plan64 = a.take<CoarsePlan<double>>(1);
     h->plan32 = a.take<CoarsePlan<float>>(1);
     h->partials = a.take<double>(2 * maxblocks);
@@ -128,6 +129,42 @@ pgmg_status wrap_level(pgmg_handle* h, int l) {
     if (!g.prd) return PGMG_OK;
     LAUNCH(nblk(halo_cells(g)), kBlock, k_halo_wrap<T>, g, view<T>(h->L[l]).x);
     return PGMG_OK;
+}
+
+// All sweeps of one leg on level l in one cooperative launch (k_sweeps_grid).
+template <class T>
+pgmg_status grid_sweeps(pgmg_handle* h, int l, int mode, int sweeps, unsigned extra = 0) {
+    Level& L = h->L[l];
+    View<T> v = view<T>(L);
+    const LevelGeom& g = L.g;
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    long need = nblk(nc, 512);
+    int cap = h->grid_blocks[std::is_same<T, float>::value ? 1 : 0];
+    int blocks = (int)(need < cap ? need : cap);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    h->launches++;
+    CK(cudaLaunchKernelEx(&cfg, k_sweeps_grid<T>, g, v.x, (const T*)v.r, (const T*)v.A, sweeps, mode, h->bar,
+                          (unsigned)blocks + extra));
+    return PGMG_OK;
+}
+
+// A persistent-sweep wait that ran out (reported once, then cleared).
+pgmg_status check_grid(pgmg_handle* h) {
+    if (!h->grid_max) return PGMG_OK;
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, &h->bar->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (!e) return PGMG_OK;
+    CK(cudaMemsetAsync(h->bar, 0, sizeof(GridBar), h->stream));
+    return fail(h, PGMG_ERR_TIMEOUT, "a grid barrier of the persistent sweep kernel ran out of time");
 }
 
 template <class T>
@@ -182,6 +219,9 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         return PGMG_OK;
     }
     int S = slab_count(g, (int)sizeof(T), h->slab_budget);
+    if (S == 1 && !g.prd && g.npts <= h->grid_max && sweeps > 0 &&
+        h->grid_blocks[std::is_same<T, float>::value ? 1 : 0] > 0)
+        return grid_sweeps<T>(h, l, mode, sweeps);
     for (int s = 0; s < sweeps; s++)
         for (int pass = 0; pass < (mode ? 2 : 1); pass++)
             for (int ss = 0; ss < S; ss++) {
@@ -582,6 +622,17 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     h->coarse_first = h->nl - 1;
     for (int l = 0; l < h->nl; l++)
         if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
+    {
+        int dev_sms = 0, nb64 = 0, nb32 = 0;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb64, k_sweeps_grid<double>, 512, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb32, k_sweeps_grid<float>, 512, 0) != cudaSuccess) {
+            cudaGetLastError();
+            nb64 = nb32 = 0;
+        }
+        h->grid_blocks[0] = nb64 * dev_sms;
+        h->grid_blocks[1] = nb32 * dev_sms;
+    }
     if (h->prd) {
         // Periodic levels keep their halo images current between kernels
         // (k_halo_wrap), so they run with the per-level kernels only.
@@ -623,7 +674,7 @@ pgmg_status pgmg_dev_set_stream(pgmg_handle* h, void* s) {
 pgmg_status pgmg_dev_sync(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     CK(cudaStreamSynchronize(h->stream));
-    return PGMG_OK;
+    return check_grid(h);
 }
 
 const char* pgmg_dev_last_error(pgmg_handle* h) { return h ? h->err : "null handle"; }
@@ -657,6 +708,12 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_PDL:
             h->pdl = value != 0;
             break;
+        case PGMG_OPT_GRID_MAX:
+            if (value < 0) return fail(h, PGMG_ERR_ARG, "grid_max must be >= 0");
+            if (value && (h->grid_blocks[0] == 0 || h->grid_blocks[1] == 0))
+                return fail(h, PGMG_ERR_UNSUPPORTED, "persistent sweep kernel not launchable");
+            h->grid_max = value;
+            break;
         case PGMG_OPT_GS_BLOCK:
             if (value != 128 && value != 256 && value != 512)
                 return fail(h, PGMG_ERR_ARG, "colour-sweep block must be 128, 256 or 512 threads");
@@ -688,6 +745,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_V_BOTTOM: *value = h->v_bottom; return PGMG_OK;
         case PGMG_OPT_PDL: *value = h->pdl; return PGMG_OK;
         case PGMG_OPT_GS_BLOCK: *value = h->gs_block; return PGMG_OK;
+        case PGMG_OPT_GRID_MAX: *value = h->grid_max; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -981,6 +1039,7 @@ struct TuneKey {
 };
 struct TuneVal {
     int gs_block, coarse_first, cluster_size, pdl;
+    long long grid_max;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -991,6 +1050,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->coarse_first = v.coarse_first;
     h->cluster_size = v.cluster_size;
     h->pdl = v.pdl != 0;
+    h->grid_max = v.grid_max;
     drop_graphs(h);
 }
 
@@ -1004,6 +1064,7 @@ pgmg_status time_vcycles(pgmg_handle* h, int reps, cudaEvent_t e0, cudaEvent_t e
     for (int i = 0; i < reps; i++) TRY(pgmg_dev_vcycle(h, 0, -1));
     CK(cudaEventRecord(e1, h->stream));
     CK(cudaEventSynchronize(e1));
+    TRY(check_grid(h));
     float t = 0;
     CK(cudaEventElapsedTime(&t, e0, e1));
     *ms = t / reps;
@@ -1013,6 +1074,19 @@ pgmg_status time_vcycles(pgmg_handle* h, int reps, cudaEvent_t e0, cudaEvent_t e
 }  // namespace
 
 extern "C" {
+
+pgmg_status pgmg_dev_grid_check(pgmg_handle* h, int level, int run_out) {
+    TRY(check_level(h, level));
+    if (h->grid_blocks[0] == 0) return fail(h, PGMG_ERR_UNSUPPORTED, "persistent sweep kernel not launchable");
+    if (h->L[level].g.prd) return fail(h, PGMG_ERR_UNSUPPORTED, "periodic level");
+    long long keep = h->grid_max;
+    h->grid_max = 1;  // makes check_grid read the error word
+    h->x0_zero = false;
+    pgmg_status st = grid_sweeps<double>(h, level, 0, 1, run_out ? 1u : 0u);
+    if (st == PGMG_OK) st = check_grid(h);
+    h->grid_max = keep;
+    return st;
+}
 
 pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     if (!h) return PGMG_ERR_ARG;
@@ -1039,12 +1113,13 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, 0};
+    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, h->grid_max, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
         double t = 0;
         pgmg_status s2 = time_vcycles(h, reps, e0, e1, &t);
+        if (s2 == PGMG_ERR_TIMEOUT) return PGMG_OK;  // a candidate that fails is not kept
         if (s2 != PGMG_OK) return s2;
         c.ms = t;
         if (t < best.ms) best = c;
@@ -1071,6 +1146,15 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
             TuneVal c = best;
             c.cluster_size = other;
             st = trial(c);
+        }
+    }
+    if (st == PGMG_OK && mc8 && !h->prd && h->grid_blocks[0] > 0 && h->grid_blocks[1] > 0) {
+        long long g0 = best.grid_max;
+        for (long long gm : {0LL, 300000LL, 3000000LL, 30000000LL}) {
+            if (gm == g0) continue;
+            TuneVal c = best;
+            c.grid_max = gm;
+            if ((st = trial(c)) != PGMG_OK) break;
         }
     }
     if (st == PGMG_OK) {
@@ -1163,7 +1247,7 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result,
     if (result) *result = st;
     if (res2) *res2 = res;
     if (cycles) *cycles = nc;
-    return PGMG_OK;
+    return check_grid(h);
 }
 
 // Residual-check schedule of the relative-residual solve.  check_every >= 1:
@@ -1291,7 +1375,7 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
     }
     if (cycles) *cycles = nc;
     if (relres) *relres = rr;
-    return PGMG_OK;
+    return check_grid(h);
 }
 
 }  // extern "C"

@@ -7,6 +7,7 @@
 #include "../../include/pgmg_dev.h"
 #include "kernels_coarse.cuh"
 #include "kernels_core.cuh"
+#include "kernels_grid.cuh"
 #include "kernels_setup.cuh"
 #include "layout.cuh"
 
@@ -98,7 +99,13 @@ struct pgmg_handle {
     bool use_graphs = true;
     int prd = 0;      // periodic axes of the problem (bit 0 x, 1 y, 2 z)
     bool pdl = true;
-    int gs_block = 256;  // threads per block of the colour sweep  // V-cycle and solve-loop kernels as programmatic dependent launches
+    int gs_block = 256;  // threads per block of the colour sweep
+    // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
+    // cluster levels with at most grid_max points (0 = off); co-resident
+    // blocks of 512 threads per precision (0 = not launchable).
+    long long grid_max = 0;
+    int grid_blocks[2] = {0, 0};
+    pgmg::GridBar* bar = nullptr;  // V-cycle and solve-loop kernels as programmatic dependent launches
     // One-cluster coarse cycle: CTAs per cluster (0 = unavailable) and the
     // first level it handles.
     int cluster_size = 0;

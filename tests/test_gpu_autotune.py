@@ -49,3 +49,37 @@ def test_gs_block_bitwise(block):
         A.v_cycle(0)
         B.v_cycle(0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+def test_grid_sweeps_bitwise_and_bounded_wait():
+    """The persistent whole-GPU sweeps give the per-pass launches' iterates bit
+    for bit; a grid barrier whose wait runs out (it waits for one block more
+    than the launch has) ends with PGMG_ERR_TIMEOUT and the device stays
+    usable."""
+    mno = (129, 97, 65)
+    A = make(mno, P.FP64)
+    B = make(mno, P.FP64)
+    B.set_option(P.OPT_GRID_MAX, 10 ** 8)  # every level above the cluster levels
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+    assert P.lib().pgmg_dev_grid_check(B.handle, 1, 0) == 0
+    assert P.lib().pgmg_dev_grid_check(B.handle, 1, 1) == 9
+    assert P.lib().pgmg_dev_grid_check(B.handle, 1, 0) == 0
+    B.clear_x(0)
+    A.clear_x(0)
+    A.solve(1e-10, 100, 1)
+    B.solve(1e-10, 100, 1)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_grid_sweeps_solve_bitwise(precision):
+    mno = (97, 97, 97)
+    A = make(mno, precision)
+    B = make(mno, precision)
+    B.set_option(P.OPT_GRID_MAX, 10 ** 8)
+    A.solve(1e-10, 100, 0)
+    B.solve(1e-10, 100, 0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
