@@ -166,7 +166,8 @@ enum {
     PGMG_OPT_V_BOTTOM = 7,
     PGMG_OPT_PDL = 8,
     PGMG_OPT_GS_BLOCK = 9,
-    PGMG_OPT_GRID_MAX = 10
+    PGMG_OPT_GRID_MAX = 10,
+    PGMG_OPT_CHECK_EVERY = 11
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
@@ -341,7 +342,12 @@ pgmg_status pgmg_batch_begin(pgmg_batch *b, int slot);
 pgmg_status pgmg_batch_step(pgmg_batch *b, double tol, int max_cycles, int *n_active);
 pgmg_status pgmg_batch_poll(pgmg_batch *b, int *active, int *cycles, double *relres);
 pgmg_status pgmg_batch_set_graphs(pgmg_batch *b, int on);
-/* PGMG_OPT_GRAPHS and PGMG_OPT_PDL for the batch's step launches. */
+/* PGMG_OPT_GRAPHS and PGMG_OPT_PDL for the batch's step launches, and
+ * PGMG_OPT_CHECK_EVERY: the residual-check period of every problem in cycles
+ * (default 1, each problem's iterates those of pgmg_dev_solve_relres with
+ * check_every = 1), or 0 for the adaptive schedule of pgmg_dev_solve_relres
+ * (in mixed precision the FP32 V-cycles between checks form one refinement
+ * step), evaluated per problem on the device. */
 pgmg_status pgmg_batch_set_option(pgmg_batch *b, int key, long long value);
 
 /* ---- host problem generators (no GPU needed) ---------------------------- */

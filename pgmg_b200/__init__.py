@@ -30,6 +30,7 @@ OPT_V_DOWN, OPT_V_UP, OPT_V_BOTTOM = 5, 6, 7
 OPT_PDL = 8
 OPT_GS_BLOCK = 9
 OPT_GRID_MAX = 10
+OPT_CHECK_EVERY = 11
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -505,7 +506,8 @@ class Batch:
         self._ck(lib().pgmg_batch_set_graphs(self._b, int(on)), "batch_set_graphs")
 
     def set_option(self, key: int, value: int):
-        """OPT_GRAPHS or OPT_PDL for the batch's step launches."""
+        """OPT_GRAPHS or OPT_PDL for the batch's step launches, OPT_CHECK_EVERY
+        for its residual-check schedule (1 = every cycle, 0 = adaptive)."""
         self._ck(lib().pgmg_batch_set_option(self._b, int(key), int(value)), "batch_set_option")
 
     @property

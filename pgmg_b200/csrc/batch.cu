@@ -127,12 +127,13 @@ __global__ void __launch_bounds__(kBlock) kb_interp(const BSlot<T>* __restrict__
 // stores it as the FP32 correction source when TO = float.
 template <class T, class TO>
 __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
-                                                   const int* __restrict__ active, const int* __restrict__ first) {
+                                                   const int* __restrict__ active, const int* __restrict__ first,
+                                                   const int* __restrict__ due) {
     pdl_enter();
     __shared__ double sh[64];
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
-    if (!active[s]) return;
+    if (!active[s] || !due[s]) return;
     const BSlot<T>& B = S[s];
     const LevelGeom& g = B.g[0];
     long nc = (long)g.M2 * g.N2 * g.O2;
@@ -159,19 +160,61 @@ __global__ void __launch_bounds__(kBlock) kb_check(const BSlot<T>* __restrict__ 
     }
 }
 
-// One block per problem: the reduction of k_reduce_partials, then the
-// convergence decision of pgmg_dev_solve_relres: stop when the relative
-// residual is below tol (or NaN, or the cycle budget is spent), otherwise
-// count the cycle that is about to run.
+// Per-problem residual-check schedule, on the device: the cycle of the next
+// check and the history the prediction uses (pgmg_dev_solve_relres's
+// CheckPlan, one per slot; rho0 is the mean reduction of the slot's last
+// solve).
+struct BPlan {
+    int next, first_n, prev_n, last_n;
+    double first_r, prev_r, last_r, rho0;
+};
+
+__device__ inline void bplan_reset(BPlan& P) {
+    P.next = 0;
+    P.first_n = P.prev_n = P.last_n = -1;
+    P.first_r = P.prev_r = P.last_r = 0;
+}
+
+// Cycle of the next check after a check at cycle nc (same rules as the
+// single-problem schedule).
+__device__ inline int bplan_next(const BPlan& P, int every, int mixed, int nc, double tol, int max_cycles) {
+    int nx;
+    double q = (P.prev_n >= 0 && P.last_r > 0 && P.prev_r > 0)
+                   ? pow(P.last_r / P.prev_r, 1.0 / (P.last_n - P.prev_n)) : P.rho0;
+    if (every >= 1) {
+        nx = nc + every;
+    } else if (!(q > 0) || q >= 0.9 || !(P.last_r > 0)) {
+        nx = nc + 1;
+    } else {
+        int n = (int)ceil(log(tol / P.last_r) / log(q));
+        if (n < 1) n = 1;
+        if (n > 1 && P.last_r * pow(q, n - 1) < kSlack * tol) n--;
+        nx = nc + n;
+        if (mixed) {
+            int cap = (int)floor(log(kInnerReduction) / log(q));
+            cap = cap < 1 ? 1 : cap > kInnerMax ? kInnerMax : cap;
+            if (nx > nc + cap) nx = nc + cap;
+        }
+    }
+    if (nx > max_cycles) nx = max_cycles;
+    if (nx < nc + 1) nx = nc + 1;
+    return nx;
+}
+
+// One block per problem due for a check: the reduction of
+// k_reduce_partials, then the convergence decision of pgmg_dev_solve_relres:
+// stop when the relative residual is below tol (or NaN, or the cycle budget
+// is spent), otherwise schedule the next check.
 template <class T>
 __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
                                                   int* __restrict__ active, int* __restrict__ first,
-                                                  int* __restrict__ cycles, double* __restrict__ relres,
-                                                  double tol, int max_cycles) {
+                                                  const int* __restrict__ cycles, double* __restrict__ relres,
+                                                  BPlan* __restrict__ plans, const int* __restrict__ due,
+                                                  double tol, int max_cycles, int every, int mixed) {
     pdl_enter();
     __shared__ double sh[64];
     int s = M->slot[blockIdx.x];
-    if (!active[s]) return;
+    if (!active[s] || !due[s]) return;
     const BSlot<T>& B = S[s];
     const LevelGeom& g = B.g[0];
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
@@ -185,17 +228,42 @@ __global__ void __launch_bounds__(1024) kb_reduce(const BSlot<T>* __restrict__ S
         double rr = b > 0 ? sqrt(a / b) : sqrt(a);
         relres[s] = rr;
         first[s] = 0;
-        if (isnan(rr) || rr < tol || cycles[s] >= max_cycles) active[s] = 0;
-        else cycles[s]++;
+        BPlan& P = plans[s];
+        int nc = cycles[s];
+        if (isnan(rr) || rr < tol || nc >= max_cycles) {
+            active[s] = 0;
+            if (nc > P.first_n && P.first_n >= 0 && P.first_r > 0 && rr > 0) {
+                double q = pow(rr / P.first_r, 1.0 / (nc - P.first_n));
+                if (q > 0 && q < 0.9) P.rho0 = q;
+            }
+        } else {
+            if (P.first_n < 0) { P.first_n = nc; P.first_r = rr; }
+            P.prev_n = P.last_n; P.prev_r = P.last_r; P.last_n = nc; P.last_r = rr;
+            P.next = bplan_next(P, every, mixed, nc, tol, max_cycles);
+        }
     }
 }
 
+// After the step's V-cycle: count it, and mark the problems whose next step
+// starts with a check (their correction is complete).
+__global__ void kb_advance(const BMap* __restrict__ M, const int* __restrict__ active, int* __restrict__ cycles,
+                           const BPlan* __restrict__ plans, int* __restrict__ due) {
+    pdl_enter();
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M->n) return;
+    int s = M->slot[e];
+    if (!active[s]) return;
+    int c = cycles[s] + 1;
+    cycles[s] = c;
+    due[s] = c >= plans[s].next;
+}
+
 __global__ void __launch_bounds__(kBlock) kb_clear32(const BSlot<float>* __restrict__ S, const BMap* __restrict__ M,
-                                                     const int* __restrict__ active) {
+                                                     const int* __restrict__ active, const int* __restrict__ due) {
     pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
-    if (!active[s]) return;
+    if (!active[s] || !due[s]) return;
     const LevelGeom& g = S[s].g[0];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
@@ -205,11 +273,11 @@ __global__ void __launch_bounds__(kBlock) kb_clear32(const BSlot<float>* __restr
 }
 
 __global__ void __launch_bounds__(kBlock) kb_add32(const BSlot<float>* __restrict__ S, const BMap* __restrict__ M,
-                                                   const int* __restrict__ active) {
+                                                   const int* __restrict__ active, const int* __restrict__ due) {
     pdl_enter();
     int e = map_entry(M, blockIdx.x);
     int s = M->slot[e];
-    if (!active[s]) return;
+    if (!active[s] || !due[s]) return;
     const LevelGeom& g = S[s].g[0];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
     if (q >= g.npts) return;
@@ -232,7 +300,8 @@ __global__ void __launch_bounds__(kBlock) kb_clear64(const BSlot<double>* S64, c
     x64[g.xi(i, j, k)] = 0.0;
 }
 
-__global__ void kb_reset(const BMap* __restrict__ M, int* active, int* first, int* cycles, double* relres) {
+__global__ void kb_reset(const BMap* __restrict__ M, int* active, int* first, int* cycles, double* relres,
+                         BPlan* plans, int* due, const double* __restrict__ rho0) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M->n) return;
     int s = M->slot[e];
@@ -240,17 +309,25 @@ __global__ void kb_reset(const BMap* __restrict__ M, int* active, int* first, in
     first[s] = 1;
     cycles[s] = 0;
     relres[s] = 0;
+    due[s] = 1;
+    bplan_reset(plans[s]);
+    plans[s].rho0 = rho0[s];
 }
 
-// Starts one slot: x = 0 on its level 0 and fresh flags.
+// Starts one slot: x = 0 on its level 0 and fresh flags; rho0 is the
+// problem's remembered reduction factor.
 __global__ void __launch_bounds__(kBlock) kb_begin(LevelGeom g, double* x64, int s, int* active, int* first,
-                                                   int* cycles, double* relres) {
+                                                   int* cycles, double* relres, BPlan* plans, int* due,
+                                                   double rho0) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (q == 0) {
         active[s] = 1;
         first[s] = 1;
         cycles[s] = 0;
         relres[s] = 0;
+        due[s] = 1;
+        bplan_reset(plans[s]);
+        plans[s].rho0 = rho0;
     }
     if (q >= g.npts) return;
     int i, j, k;
@@ -275,6 +352,9 @@ struct pgmg_batch {
     int* first = nullptr;
     int* cycles = nullptr;
     double* relres = nullptr;
+    BPlan* plans = nullptr;  // residual-check schedule per slot
+    double* rho_in = nullptr;  // per-slot starting reduction factors (staging)
+    int* due = nullptr;      // 1: the slot's next step starts with a check
     int* cluster_slots = nullptr;
     // shape
     bool dirty = true;
@@ -290,6 +370,7 @@ struct pgmg_batch {
     bool pdl = true;  // step kernels as programmatic dependent launches
     double cap_tol = -1;  // tol and cycle cap the step graphs were captured with
     int cap_max = -1;
+    int check_every = 1;  // residual check period in cycles, 0 = adaptive
     long long launches = 0;
     char err[512] = {0};
 };
@@ -452,12 +533,13 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
     const BSlot<T>* S = static_cast<const BSlot<T>*>(b->slot_table);
     auto M = [&](int m) { return b->maps + m; };
     using TO = T;
-    BLAUNCH(map_blocks(b, b->map_chk), kBlock, kb_check<T, TO>, S, M(b->map_chk), b->active, b->first);
+    const int mixed = std::is_same<T, float>::value ? 1 : 0;
+    BLAUNCH(map_blocks(b, b->map_chk), kBlock, kb_check<T, TO>, S, M(b->map_chk), b->active, b->first, b->due);
     BLAUNCH((int)b->members.size(), 1024, kb_reduce<T>, S, M(b->map_red), b->active, b->first, b->cycles,
-                                                                  b->relres, tol, max_cycles);
-    if (std::is_same<T, float>::value) {
-        BLAUNCH(map_blocks(b, b->map_pt0), kBlock, kb_clear32, 
-            reinterpret_cast<const BSlot<float>*>(S), M(b->map_pt0), b->active);
+            b->relres, b->plans, b->due, tol, max_cycles, b->check_every, mixed);
+    if (mixed) {
+        BLAUNCH(map_blocks(b, b->map_pt0), kBlock, kb_clear32, reinterpret_cast<const BSlot<float>*>(S),
+                M(b->map_pt0), b->active, b->due);
     }
     for (int l = 0; l < b->maxtop; l++) {
         if (b->map_gs[l] < 0) continue;
@@ -496,9 +578,11 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
                 BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, c);
             }
     }
-    if (std::is_same<T, float>::value) {
+    int nm = (int)b->members.size();
+    BLAUNCH((nm + 127) / 128, 128, kb_advance, M(b->map_red), b->active, b->cycles, b->plans, b->due);
+    if (mixed) {
         BLAUNCH(map_blocks(b, b->map_pt0), kBlock, kb_add32, reinterpret_cast<const BSlot<float>*>(S),
-                                                                        M(b->map_pt0), b->active);
+                M(b->map_pt0), b->active, b->due);
     }
     return PGMG_OK;
 }
@@ -572,7 +656,12 @@ pgmg_status batch_solve(pgmg_batch* b, double tol, int max_cycles, int* cycles, 
     }
     if (b->members.empty()) return PGMG_OK;
     int nm = (int)b->members.size();
-    kb_reset<<<(nm + 127) / 128, 128, 0, b->stream>>>(b->maps + b->map_red, b->active, b->first, b->cycles, b->relres);
+    // Each problem starts from its handle's remembered reduction factor.
+    std::vector<double> rho(kMaxSlots, 0.0);
+    for (int s : b->members) rho[s] = b->slots[s]->last_rho;
+    BCK(cudaMemcpyAsync(b->rho_in, rho.data(), sizeof(double) * kMaxSlots, cudaMemcpyHostToDevice, b->stream));
+    kb_reset<<<(nm + 127) / 128, 128, 0, b->stream>>>(b->maps + b->map_red, b->active, b->first, b->cycles, b->relres,
+                                                    b->plans, b->due, b->rho_in);
     BKL();
     kb_clear64<<<map_blocks(b, b->map_pt0), kBlock, 0, b->stream>>>(
         std::is_same<T, double>::value ? static_cast<const BSlot<double>*>(b->slot_table) : nullptr,
@@ -587,9 +676,12 @@ pgmg_status batch_solve(pgmg_batch* b, double tol, int max_cycles, int* cycles, 
     }
     std::vector<int> cyc(kMaxSlots);
     std::vector<double> rr(kMaxSlots);
+    std::vector<BPlan> pl(kMaxSlots);
     BCK(cudaMemcpyAsync(cyc.data(), b->cycles, sizeof(int) * kMaxSlots, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaMemcpyAsync(rr.data(), b->relres, sizeof(double) * kMaxSlots, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaMemcpyAsync(pl.data(), b->plans, sizeof(BPlan) * kMaxSlots, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
+    for (int s : b->members) b->slots[s]->last_rho = pl[s].rho0;  // learned, for the problem's next solve
     for (int s = 0; s < (int)b->slots.size(); s++) {
         if (cycles) cycles[s] = b->slots[s] ? cyc[s] : 0;
         if (relres) relres[s] = b->slots[s] ? rr[s] : 0;
@@ -624,6 +716,9 @@ pgmg_status pgmg_batch_create(int max_slots, int precision, int device, pgmg_bat
         cudaMalloc(&b->first, sizeof(int) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->cycles, sizeof(int) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->relres, sizeof(double) * kMaxSlots) != cudaSuccess ||
+        cudaMalloc(&b->plans, sizeof(BPlan) * kMaxSlots) != cudaSuccess ||
+        cudaMalloc(&b->rho_in, sizeof(double) * kMaxSlots) != cudaSuccess ||
+        cudaMalloc(&b->due, sizeof(int) * kMaxSlots) != cudaSuccess ||
         cudaMalloc(&b->cluster_slots, sizeof(int) * kMaxSlots) != cudaSuccess) {
         cudaGetLastError();
         pgmg_batch_destroy(b);
@@ -632,6 +727,8 @@ pgmg_status pgmg_batch_create(int max_slots, int precision, int device, pgmg_bat
     cudaMemsetAsync(b->active, 0, sizeof(int) * kMaxSlots, b->stream);
     cudaMemsetAsync(b->first, 0, sizeof(int) * kMaxSlots, b->stream);
     cudaMemsetAsync(b->cycles, 0, sizeof(int) * kMaxSlots, b->stream);
+    cudaMemsetAsync(b->plans, 0, sizeof(BPlan) * kMaxSlots, b->stream);
+    cudaMemsetAsync(b->due, 0, sizeof(int) * kMaxSlots, b->stream);
     cudaStreamSynchronize(b->stream);
     *out = b;
     return PGMG_OK;
@@ -648,6 +745,9 @@ pgmg_status pgmg_batch_destroy(pgmg_batch* b) {
     cudaFree(b->first);
     cudaFree(b->cycles);
     cudaFree(b->relres);
+    cudaFree(b->plans);
+    cudaFree(b->rho_in);
+    cudaFree(b->due);
     cudaFree(b->cluster_slots);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -678,6 +778,13 @@ pgmg_status pgmg_batch_attach(pgmg_batch* b, int slot, pgmg_handle* h) {
 
 pgmg_status pgmg_batch_detach(pgmg_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->slots.size()) return PGMG_ERR_ARG;
+    if (b->slots[slot]) {
+        // The reduction factor the slot learned goes back to its problem.
+        BPlan p;
+        BCK(cudaMemcpyAsync(&p, b->plans + slot, sizeof(BPlan), cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        b->slots[slot]->last_rho = p.rho0;
+    }
     BCK(cudaMemsetAsync(b->active + slot, 0, sizeof(int), b->stream));
     b->slots[slot] = nullptr;
     b->dirty = true;
@@ -689,7 +796,8 @@ pgmg_status pgmg_batch_begin(pgmg_batch* b, int slot) {
     pgmg_handle* h = b->slots[slot];
     BCK(cudaStreamSynchronize(h->stream));  // its set-up and source are complete
     const LevelGeom& g = h->L[0].g;
-    kb_begin<<<nblk(g.npts), kBlock, 0, b->stream>>>(g, h->L[0].x64, slot, b->active, b->first, b->cycles, b->relres);
+    kb_begin<<<nblk(g.npts), kBlock, 0, b->stream>>>(g, h->L[0].x64, slot, b->active, b->first, b->cycles, b->relres,
+                                                     b->plans, b->due, h->last_rho);
     BKL();
     h->x0_zero = false;
     return PGMG_OK;
@@ -723,6 +831,10 @@ pgmg_status pgmg_batch_set_option(pgmg_batch* b, int key, long long value) {
     switch (key) {
         case PGMG_OPT_GRAPHS: b->use_graphs = value != 0; break;
         case PGMG_OPT_PDL: b->pdl = value != 0; break;
+        case PGMG_OPT_CHECK_EVERY:
+            if (value < 0) return bfail(b, PGMG_ERR_ARG, "check period must be >= 0");
+            b->check_every = (int)value;
+            break;
         default: return bfail(b, PGMG_ERR_ARG, "unknown batch option %d", key);
     }
     drop_step_graphs(b);

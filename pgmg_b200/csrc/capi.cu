@@ -1256,7 +1256,6 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result,
 // the handle's previous solve) and the solve runs the cycles predicted to
 // reach tol before checking again, stopping one short when that one might
 // already be enough.
-constexpr double kSlack = 3.0;
 
 struct CheckPlan {
     int every;
@@ -1287,10 +1286,6 @@ struct CheckPlan {
     }
 };
 
-// Mixed precision: the largest reduction asked of the FP32 V-cycles of one
-// refinement step, and the most cycles one step runs.
-constexpr double kInnerReduction = 1e-5;
-constexpr int kInnerMax = 16;
 
 pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
                                   double* relres) {

@@ -19,6 +19,13 @@ constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicograp
 constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
 constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
 constexpr int kClusterThreads = 512;
+// Residual-check schedule (single solves and batches): check one cycle
+// before the predicted count when that cycle's predicted residual is within
+// kSlack of tol.  Mixed precision: the largest reduction asked of the FP32
+// V-cycles of one refinement step, and the most cycles one step runs.
+constexpr double kSlack = 3.0;
+constexpr double kInnerReduction = 1e-5;
+constexpr int kInnerMax = 16;
 
 struct Level {
     LevelGeom g;

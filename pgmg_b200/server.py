@@ -35,7 +35,7 @@ import time
 
 import numpy as np
 
-from . import (MIXED, Batch, Multigrid, PgmgError, plan_bytes, problem_gauss)
+from . import (MIXED, OPT_CHECK_EVERY, Batch, Multigrid, PgmgError, plan_bytes, problem_gauss)
 
 
 @dataclasses.dataclass
@@ -135,7 +135,7 @@ class _Resident:
 class SolveServer:
     def __init__(self, cap_bytes: float, max_slots: int = 64, precision: int = MIXED, tol: float = 1e-10,
                  max_cycles: int = 100, device: int = 0, keep_solutions: bool = False, fields: FieldPool | None = None,
-                 setup_threads: int = 4):
+                 setup_threads: int = 4, check_every: int = 0):
         self.cap = int(cap_bytes)
         self.max_slots = max_slots
         self.precision = precision
@@ -150,6 +150,9 @@ class SolveServer:
         self.pool = DevicePool(self.cap, device)
         self.fields = fields or FieldPool(device)
         self.batch = Batch(max_slots, precision, device)
+        # Residual checks per problem: 0 = the adaptive schedule (several
+        # FP32 V-cycles per refinement step), 1 = every cycle.
+        self.batch.set_option(OPT_CHECK_EVERY, check_every)
         self.resident = collections.OrderedDict()  # pid -> _Resident (LRU order)
         self.free_slots = list(range(max_slots))
         self.running = {}  # slot -> (request, resident)

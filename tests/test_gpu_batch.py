@@ -57,3 +57,36 @@ def test_batch_rejects_unsupported():
     with pytest.raises(P.PgmgError):
         B.attach(0, G2)  # lexicographic smoother
     B.close()
+
+
+@pytest.mark.parametrize("precision", [P.MIXED, P.FP64])
+def test_batch_adaptive_schedule(precision):
+    """Adaptive residual checks, per problem on the device: every problem
+    converges, fewer checks than cycles are paid, and a problem's result is
+    the same in the mix and in a batch of its own."""
+    probs = [build(s, precision, 30 + i) for i, s in enumerate(SHAPES)]
+    B = P.Batch(8, precision)
+    B.set_option(P.OPT_CHECK_EVERY, 0)
+    for s, G in enumerate(probs):
+        B.attach(s, G)
+    cyc, rr = B.solve(1e-10, 60)
+    xb = [G.get_x(0) for G in probs]
+    for s, G in enumerate(probs):
+        assert rr[s] < 1e-10 and cyc[s] > 0
+        # Close to the problem's own FP64-checked solve.
+        H = build(SHAPES[s], precision, 30 + s)
+        H.solve(1e-12, 80, 1)
+        xh = H.get_x(0)
+        assert np.abs(xb[s] - xh).max() / np.abs(xh).max() < 1e-8
+    B.close()
+    # The same problems, fresh (same starting state), each in a batch of its
+    # own: the same result as in the mix.
+    for s in (0, 3, 7):
+        G = build(SHAPES[s], precision, 30 + s)
+        C = P.Batch(2, precision)
+        C.set_option(P.OPT_CHECK_EVERY, 0)
+        C.attach(1, G)
+        c1, r1 = C.solve(1e-10, 60)
+        assert c1[1] == cyc[s] and r1[1] == rr[s]
+        assert np.array_equal(G.get_x(0), xb[s])
+        C.close()
