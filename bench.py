@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--batch-problems", type=int, default=96, help="problems in the batch96 workload")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-seq-seconds", type=float, default=60.0,
+                    help="time budget of the one-request-at-a-time comparison")
     return ap.parse_args()
 
 
@@ -657,10 +659,15 @@ def run_serve(a):
     srv.close()
     del srv
     torch.cuda.empty_cache()
-    # The same requests one at a time (set-up when not resident, then a solve).
+    # The same requests one at a time (set-up when not resident, then a
+    # solve), in arrival order, for at most --serve-seq-seconds.
     cache = {}
     t0 = time.perf_counter()
+    nseq = 0
     for r in reqs:
+        if time.perf_counter() - t0 > a.serve_seq_seconds:
+            break
+        nseq += 1
         G = cache.get(r.problem)
         if G is None:
             G = P.Multigrid(*r.shape, precision=P.MIXED)
@@ -675,7 +682,8 @@ def run_serve(a):
         G.clear_x(0)
         G.solve(1e-10, 100, 0)
     seq = time.perf_counter() - t0
-    out["sequential"] = {"value": len(reqs) / seq, "unit": "solves/s", "s": seq}
+    out["sequential"] = {"value": nseq / seq, "unit": "solves/s", "s": seq,
+                         "sample": f"the first {nseq} of the {len(reqs)} requests"}
     out["speedup_vs_sequential"] = out["value"] / out["sequential"]["value"]
     print(json.dumps(out))
 
