@@ -146,6 +146,11 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           dependent launches, so that each is scheduled while
  *                           the one before it drains (default); 0 = plain
  *                           launches.  No counterpart in the reference.
+ *   PGMG_OPT_GS_VECTOR      1 = the 8-colour sweep kernel updates 2 (FP64) or
+ *                           4 (FP32) consecutive colour points per thread with
+ *                           128-bit loads of their stencil coefficients; 0 =
+ *                           one point per thread (default).  No counterpart in
+ *                           the reference.
  *   PGMG_OPT_GS_BLOCK       threads per block of the 8-colour sweep kernel:
  *                           128, 256 (default) or 512.  No counterpart in the
  *                           reference.
@@ -167,13 +172,15 @@ enum {
     PGMG_OPT_PDL = 8,
     PGMG_OPT_GS_BLOCK = 9,
     PGMG_OPT_GRID_MAX = 10,
-    PGMG_OPT_CHECK_EVERY = 11
+    PGMG_OPT_CHECK_EVERY = 11,
+    PGMG_OPT_GS_VECTOR = 12
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
- * PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_GRID_MAX, PGMG_OPT_PDL -- one at a time from the best so
+ * PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_GRID_MAX, PGMG_OPT_PDL --
+ * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,
  * precision, smoother, device): a later handle of the same shape takes it

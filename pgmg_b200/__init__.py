@@ -31,6 +31,7 @@ OPT_PDL = 8
 OPT_GS_BLOCK = 9
 OPT_GRID_MAX = 10
 OPT_CHECK_EVERY = 11
+OPT_GS_VECTOR = 12
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -277,7 +278,7 @@ class Multigrid:
         self._ck(lib().pgmg_dev_autotune(self._h, int(reps), C.byref(ms)), "autotune")
         return {"gs_block": self.get_option(OPT_GS_BLOCK), "cluster_first": self.get_option(OPT_CLUSTER_FIRST),
                 "cluster_size": self.get_option(OPT_CLUSTER_SIZE), "pdl": self.get_option(OPT_PDL),
-                "grid_max": self.get_option(OPT_GRID_MAX),
+                "grid_max": self.get_option(OPT_GRID_MAX), "gs_vector": self.get_option(OPT_GS_VECTOR),
                 "vcycle_ms": ms.value}
 
     def set_smoother(self, smoother: int):

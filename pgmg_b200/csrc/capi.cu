@@ -219,6 +219,23 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         return PGMG_OK;
     }
     int S = slab_count(g, (int)sizeof(T), h->slab_budget);
+    if (S == 1 && !g.prd && h->gs_vec) {
+        // 16-byte vector loads, V colour points per thread.
+        constexpr int V = 16 / sizeof(T);
+        long nthr = ((long)g.M2 * g.N2 * g.O2 + V - 1) / V;
+        for (int s = 0; s < sweeps; s++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = pass ? 7 - cc : cc;
+                    if (h->gs_block == 128)
+                        LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col);
+                    else if (h->gs_block == 512)
+                        LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col);
+                    else
+                        LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col);
+                }
+        return PGMG_OK;
+    }
     if (S == 1 && !g.prd && g.npts <= h->grid_max && sweeps > 0 &&
         h->grid_blocks[std::is_same<T, float>::value ? 1 : 0] > 0)
         return grid_sweeps<T>(h, l, mode, sweeps);
@@ -708,6 +725,9 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_PDL:
             h->pdl = value != 0;
             break;
+        case PGMG_OPT_GS_VECTOR:
+            h->gs_vec = value != 0;
+            break;
         case PGMG_OPT_GRID_MAX:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "grid_max must be >= 0");
             if (value && (h->grid_blocks[0] == 0 || h->grid_blocks[1] == 0))
@@ -746,6 +766,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_PDL: *value = h->pdl; return PGMG_OK;
         case PGMG_OPT_GS_BLOCK: *value = h->gs_block; return PGMG_OK;
         case PGMG_OPT_GRID_MAX: *value = h->grid_max; return PGMG_OK;
+        case PGMG_OPT_GS_VECTOR: *value = h->gs_vec; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1040,6 +1061,7 @@ struct TuneKey {
 struct TuneVal {
     int gs_block, coarse_first, cluster_size, pdl;
     long long grid_max;
+    int gs_vec;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1051,6 +1073,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->cluster_size = v.cluster_size;
     h->pdl = v.pdl != 0;
     h->grid_max = v.grid_max;
+    h->gs_vec = v.gs_vec != 0;
     drop_graphs(h);
 }
 
@@ -1113,7 +1136,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, h->grid_max, 0};
+    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, h->grid_max, h->gs_vec ? 1 : 0, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1127,8 +1150,14 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     };
     bool mc8 = h->dims.smoother == PGMG_SMOOTH_MC8;
     // Coordinate descent: one option at a time, each from the best so far.
+    if (st == PGMG_OK && mc8 && !h->prd) {
+        TuneVal c = best;
+        c.gs_vec = !best.gs_vec;
+        st = trial(c);
+    }
     if (st == PGMG_OK && mc8 && !h->prd)
-        for (int b : {128, 512}) {
+        for (int b : {128, 256, 512}) {
+            if (b == best.gs_block) continue;
             TuneVal c = best;
             c.gs_block = b;
             if ((st = trial(c)) != PGMG_OK) break;

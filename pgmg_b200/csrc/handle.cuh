@@ -107,6 +107,7 @@ struct pgmg_handle {
     int prd = 0;      // periodic axes of the problem (bit 0 x, 1 y, 2 z)
     bool pdl = true;
     int gs_block = 256;  // threads per block of the colour sweep
+    bool gs_vec = false;  // colour sweep with 16-byte vector loads (k_gs_colour_v)
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident
     // blocks of 512 threads per precision (0 = not launchable).

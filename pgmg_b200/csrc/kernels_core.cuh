@@ -65,6 +65,54 @@ __global__ void __launch_bounds__(BS) k_gs_colour(LevelGeom g, T* x, const T* __
     gs_colour_at<T, PRD>(g, x, r, A, col, p);
 }
 
+// The same colour pass with 16-byte vector loads: each thread updates V =
+// 16/sizeof(T) consecutive colour points (2 FP64, 4 FP32), loading the V
+// points' coefficient of each stencil slot, their sources and diagonals with
+// one 128-bit load each.  Every point's arithmetic is gs_value's, in the same
+// order, so results are bit-identical to k_gs_colour.  One slab only (p
+// starts at 0, so every thread's first point is a multiple of V and its loads
+// are aligned: colour-major planes are padded to multiples of 64 points).
+template <class T, int BS>
+__global__ void __launch_bounds__(BS) k_gs_colour_v(LevelGeom g, T* x, const T* __restrict__ r,
+                                                    const T* __restrict__ A, int col) {
+    constexpr int V = 16 / sizeof(T);
+    pdl_enter();
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    long p0 = (blockIdx.x * (long)BS + threadIdx.x) * V;
+    if (p0 >= nc) return;
+    uint64_t ps = policy_evict_first(), pk = policy_evict_last();
+    const long safe = g.xi(0, 0, 0);  // a point whose 27 neighbours exist (halo)
+    long xc[V];
+    bool ok[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        int i2, j2, k2;
+        decode_colour(g, p0 + v, i2, j2, k2);
+        int i = 2 * i2 + (col & 1), j = 2 * j2 + ((col >> 1) & 1), k = 2 * k2 + (col >> 2);
+        ok[v] = p0 + v < nc && i < g.m && j < g.n && k < g.o;
+        xc[v] = ok[v] ? g.xi(i, j, k) : safe;
+    }
+    const T* Ap = A + (long)col * 27 * g.Nc + p0;
+    T acc[V];
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = T(0);
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        if (q == 13) continue;
+        T a[V];
+        ld_stream_v(Ap + q * g.Nc, ps, a);
+        long o = slot_off(g, q);
+#pragma unroll
+        for (int v = 0; v < V; v++) acc[v] = madd<true, T>(acc[v], a[v], ld_keep(x + xc[v] + o, pk));
+    }
+    T d[V], rv[V];
+    ld_stream_v(Ap + 13 * g.Nc, ps, d);
+    ld_stream_v(r + (long)col * g.Nc + p0, ps, rv);
+#pragma unroll
+    for (int v = 0; v < V; v++)
+        if (ok[v]) st_keep(x + xc[v], mul_rn<T>(sub_rn<T>(rv[v], acc[v]), T(1) / d[v]), pk);
+}
+
 // Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of
 // a 27-point box that precedes a point lexicographically lies on an earlier
 // hyperplane (offsets (-1,0,0) -> -1; (+1,-1,0) -> -1; (d,d',-1) -> <= -1)

@@ -83,3 +83,17 @@ def test_grid_sweeps_solve_bitwise(precision):
     A.solve(1e-10, 100, 0)
     B.solve(1e-10, 100, 0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+@pytest.mark.parametrize("mno", [(41, 41, 41), (33, 40, 17), (65, 20, 9)])
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_gs_vector_bitwise(mno, precision):
+    """The 16-byte-load colour sweep (2 or 4 points per thread) gives the
+    one-point-per-thread sweep's iterates bit for bit, odd sizes included."""
+    A = make(mno, precision)
+    B = make(mno, precision)
+    B.set_option(P.OPT_GS_VECTOR, 1)
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
