@@ -227,39 +227,24 @@ def run_reference(a):
 
 def run_ours(a):
     import torch
-    import torch.distributed as dist
 
     import pgmg_b200 as P
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from pgmg_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl")
+    world, rank = rep.world, rep.rank
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     m = a.size
     npts = m ** 3
     smoother = P.SMOOTH_LEX if a.smoother == "lex" else P.SMOOTH_MC8
     tg = time.perf_counter()
     if a.device_setup:
-        gfield = P.problem_gauss(m, m, m, a.seed + rank, 8.0)
+        gfield = P.problem_gauss(m, m, m, rep.seed(a.seed), 8.0)
         coef = S = None
     else:
-        coef, S, r = build_problem(m, a.sigma, a.seed + rank)
+        coef, S, r = build_problem(m, a.sigma, rep.seed(a.seed))
     gen_s = time.perf_counter() - tg
 
     stream = torch.cuda.Stream(device=dev)
@@ -270,7 +255,7 @@ def run_ours(a):
     def setup(H):
         if a.device_setup:
             H.assemble_q1(gfield, from_log=True, sigma=a.sigma)
-            H.rhs_uniform(a.seed + rank)
+            H.rhs_uniform(rep.seed(a.seed))
         else:
             H.setup_matrices(coef, S)
             H.setup_fields(r)
@@ -376,12 +361,12 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         if coef is None:
-            coef, S = P.problem_q1(m, m, m, P.problem_kappa(m, m, m, a.sigma, a.seed + rank, 8.0))
+            coef, S = P.problem_q1(m, m, m, P.problem_kappa(m, m, m, a.sigma, rep.seed(a.seed), 8.0))
         cpu = cpu_baseline(a, coef, S, r, G)
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "metric": METRIC, "value": rep.per_solve(ms) / 1e3, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded kappa field and RHS)",
             "config": {"workload": f"{m}^3 Q1 variable-kappa sigma={a.sigma} FP64, solve to {a.tol} rel residual",
@@ -389,8 +374,9 @@ def run_ours(a):
                        "smoother": ("lexicographic (wavefront) Gauss-Seidel" if a.smoother == "lex"
                                     else "8-colour Gauss-Seidel"), "coarse": "FP64 LU (explicit inverse)",
                        "l2": "inputs larger than L2 (3.7 GB stencils)", "setup_s": setup_s,
-                       "host_generation_s": gen_s, "parallelism": f"replicas x{world}", "tuning": tuning},
-            "e2e": {"value": e2e_ms / 1e3, "unit": UNIT, "h2d_bytes_per_step": npts * 8,
+                       "host_generation_s": gen_s, "parallelism": f"replicas x{world}", "tuning": tuning,
+                       "per_rank_s_per_solve": ms / 1e3},
+            "e2e": {"value": rep.per_solve(e2e_ms) / 1e3, "unit": UNIT, "h2d_bytes_per_step": npts * 8,
                     "d2h_bytes_per_step": npts * 8},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic if a.smoother == "mc8" else None,
@@ -404,8 +390,7 @@ def run_ours(a):
         }
         print(json.dumps(line), flush=True)
     G.close()
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def cpu_baseline(a, coef, S, r, G):
