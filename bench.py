@@ -247,7 +247,7 @@ def run_ours(a):
         coef, S, r = build_problem(m, a.sigma, rep.seed(a.seed))
     gen_s = time.perf_counter() - tg
 
-    stream = torch.cuda.Stream(device=dev)
+    stream = torch.cuda.Stream(device=torch.device("cuda", local))
     G = P.Multigrid(m, m, m, precision=P.FP64, coarse=P.COARSE_LU, smoother=smoother, device=local)
     G.set_stream(stream.cuda_stream)
     torch.cuda.synchronize()

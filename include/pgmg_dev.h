@@ -151,6 +151,10 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           128-bit loads of their stencil coefficients; 0 =
  *                           one point per thread (default).  No counterpart in
  *                           the reference.
+ *   PGMG_OPT_INNER_DIGITS   mixed precision, adaptive schedule: the FP32
+ *                           V-cycles of one refinement step are asked for at
+ *                           most a 10^-d predicted reduction (1..7, default 5).
+ *                           Changes the iterates (not the tolerance reached).
  *   PGMG_OPT_GS_BLOCK       threads per block of the 8-colour sweep kernel:
  *                           128, 256 (default) or 512.  No counterpart in the
  *                           reference.
@@ -173,7 +177,8 @@ enum {
     PGMG_OPT_GS_BLOCK = 9,
     PGMG_OPT_GRID_MAX = 10,
     PGMG_OPT_CHECK_EVERY = 11,
-    PGMG_OPT_GS_VECTOR = 12
+    PGMG_OPT_GS_VECTOR = 12,
+    PGMG_OPT_INNER_DIGITS = 13
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after

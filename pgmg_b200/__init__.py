@@ -32,6 +32,7 @@ OPT_GS_BLOCK = 9
 OPT_GRID_MAX = 10
 OPT_CHECK_EVERY = 11
 OPT_GS_VECTOR = 12
+OPT_INNER_DIGITS = 13
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",

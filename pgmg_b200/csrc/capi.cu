@@ -728,6 +728,10 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_GS_VECTOR:
             h->gs_vec = value != 0;
             break;
+        case PGMG_OPT_INNER_DIGITS:
+            if (value < 1 || value > 7) return fail(h, PGMG_ERR_ARG, "inner reduction digits must be 1..7");
+            h->inner_digits = (int)value;
+            break;
         case PGMG_OPT_GRID_MAX:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "grid_max must be >= 0");
             if (value && (h->grid_blocks[0] == 0 || h->grid_blocks[1] == 0))
@@ -767,6 +771,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_GS_BLOCK: *value = h->gs_block; return PGMG_OK;
         case PGMG_OPT_GRID_MAX: *value = h->grid_max; return PGMG_OK;
         case PGMG_OPT_GS_VECTOR: *value = h->gs_vec; return PGMG_OK;
+        case PGMG_OPT_INNER_DIGITS: *value = h->inner_digits; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1372,7 +1377,7 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             // limits what the correction can gain).
             int inner = next_check - nc;
             double q = plan.rho();
-            int cap = q > 0 && q < 0.9 ? (int)floor(log(kInnerReduction) / log(q)) : 1;
+            int cap = q > 0 && q < 0.9 ? (int)floor(-h->inner_digits * log(10.0) / log(q)) : 1;
             cap = cap < 1 ? 1 : cap > kInnerMax ? kInnerMax : cap;
             if (plan.every == 0 && inner > cap) inner = cap;
             if (inner > max_cycles - nc) inner = max_cycles - nc;

@@ -108,6 +108,7 @@ struct pgmg_handle {
     bool pdl = true;
     int gs_block = 256;  // threads per block of the colour sweep
     bool gs_vec = false;  // colour sweep with 16-byte vector loads (k_gs_colour_v)
+    int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident
     // blocks of 512 threads per precision (0 = not launchable).
