@@ -151,6 +151,18 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           128-bit loads of their stencil coefficients; 0 =
  *                           one point per thread (default).  No counterpart in
  *                           the reference.
+ *   PGMG_OPT_GS_ALTERNATE   1 = consecutive colour passes traverse the level in
+ *                           opposite directions, so that each starts on the
+ *                           solution planes the previous one left in L2
+ *                           (default); 0 = always bottom up.  No counterpart
+ *                           in the reference.
+ *   PGMG_OPT_GS_PREFETCH    8-colour levels of at most this many points load
+ *                           each colour pass's stencil coefficients before
+ *                           waiting for the previous kernel (with PGMG_OPT_PDL,
+ *                           so that the loads overlap that kernel's drain);
+ *                           0 = no level.  Default 4194304.  Levels that
+ *                           PGMG_OPT_GS_VECTOR or PGMG_OPT_GRID_MAX sweep keep
+ *                           those paths.  No counterpart in the reference.
  *   PGMG_OPT_INNER_DIGITS   mixed precision, adaptive schedule: the FP32
  *                           V-cycles of one refinement step are asked for at
  *                           most a 10^-d predicted reduction (1..7, default 5).
@@ -178,13 +190,16 @@ enum {
     PGMG_OPT_GRID_MAX = 10,
     PGMG_OPT_CHECK_EVERY = 11,
     PGMG_OPT_GS_VECTOR = 12,
-    PGMG_OPT_INNER_DIGITS = 13
+    PGMG_OPT_INNER_DIGITS = 13,
+    PGMG_OPT_GS_ALTERNATE = 14,
+    PGMG_OPT_GS_PREFETCH = 15
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
- * PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE, PGMG_OPT_GRID_MAX, PGMG_OPT_PDL --
+ * PGMG_OPT_GS_ALTERNATE, PGMG_OPT_GS_PREFETCH, PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE,
+ * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL --
  * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,

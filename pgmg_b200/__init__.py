@@ -33,6 +33,8 @@ OPT_GRID_MAX = 10
 OPT_CHECK_EVERY = 11
 OPT_GS_VECTOR = 12
 OPT_INNER_DIGITS = 13
+OPT_GS_ALTERNATE = 14
+OPT_GS_PREFETCH = 15
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -280,6 +282,7 @@ class Multigrid:
         return {"gs_block": self.get_option(OPT_GS_BLOCK), "cluster_first": self.get_option(OPT_CLUSTER_FIRST),
                 "cluster_size": self.get_option(OPT_CLUSTER_SIZE), "pdl": self.get_option(OPT_PDL),
                 "grid_max": self.get_option(OPT_GRID_MAX), "gs_vector": self.get_option(OPT_GS_VECTOR),
+                "gs_alternate": self.get_option(OPT_GS_ALTERNATE), "gs_prefetch": self.get_option(OPT_GS_PREFETCH),
                 "vcycle_ms": ms.value}
 
     def set_smoother(self, smoother: int):

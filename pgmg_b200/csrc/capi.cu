@@ -227,18 +227,36 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
             for (int pass = 0; pass < (mode ? 2 : 1); pass++)
                 for (int cc = 0; cc < 8; cc++) {
                     int col = pass ? 7 - cc : cc;
+                    int rev = h->gs_alt ? (cc & 1) : 0;
                     if (h->gs_block == 128)
-                        LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col);
+                        LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col, rev);
                     else if (h->gs_block == 512)
-                        LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col);
+                        LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col, rev);
                     else
-                        LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col);
+                        LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col, rev);
                 }
         return PGMG_OK;
     }
     if (S == 1 && !g.prd && g.npts <= h->grid_max && sweeps > 0 &&
         h->grid_blocks[std::is_same<T, float>::value ? 1 : 0] > 0)
         return grid_sweeps<T>(h, l, mode, sweeps);
+    if (S == 1 && !g.prd && g.npts <= h->gs_prefetch) {
+        // Stencil loaded before the launch dependency (k_gs_colour_pf).
+        long nc = (long)g.M2 * g.N2 * g.O2;
+        for (int s = 0; s < sweeps; s++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = pass ? 7 - cc : cc;
+                    int rev = h->gs_alt ? (cc & 1) : 0;
+                    if (h->gs_block == 128)
+                        LAUNCH(nblk(nc, 128), 128, k_gs_colour_pf<T, 128>, g, v.x, v.r, v.A, col, rev);
+                    else if (h->gs_block == 512)
+                        LAUNCH(nblk(nc, 512), 512, k_gs_colour_pf<T, 512>, g, v.x, v.r, v.A, col, rev);
+                    else
+                        LAUNCH(nblk(nc, 256), 256, k_gs_colour_pf<T, 256>, g, v.x, v.r, v.A, col, rev);
+                }
+        return PGMG_OK;
+    }
     for (int s = 0; s < sweeps; s++)
         for (int pass = 0; pass < (mode ? 2 : 1); pass++)
             for (int ss = 0; ss < S; ss++) {
@@ -247,16 +265,17 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 long np = (long)(k2hi - k2lo) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
                     int col = pass ? 7 - cc : cc;
+                    int rev = h->gs_alt ? (cc & 1) : 0;  // alternate the traversal direction
                     if (g.prd)
-                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
+                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi, rev);
                     else if (h->gs_block == 128)
                         LAUNCH(nblk(np, 128), 128, k_gs_colour<T, true, false, 128>, g, v.x, v.r, v.A, col, k2lo,
-                               k2hi);
+                               k2hi, rev);
                     else if (h->gs_block == 512)
                         LAUNCH(nblk(np, 512), 512, k_gs_colour<T, true, false, 512>, g, v.x, v.r, v.A, col, k2lo,
-                               k2hi);
+                               k2hi, rev);
                     else
-                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi);
+                        LAUNCH(nblk(np), kBlock, k_gs_colour<T, true>, g, v.x, v.r, v.A, col, k2lo, k2hi, rev);
                 }
             }
     return PGMG_OK;
@@ -728,6 +747,13 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_GS_VECTOR:
             h->gs_vec = value != 0;
             break;
+        case PGMG_OPT_GS_ALTERNATE:
+            h->gs_alt = value != 0;
+            break;
+        case PGMG_OPT_GS_PREFETCH:
+            if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
+            h->gs_prefetch = value;
+            break;
         case PGMG_OPT_INNER_DIGITS:
             if (value < 1 || value > 7) return fail(h, PGMG_ERR_ARG, "inner reduction digits must be 1..7");
             h->inner_digits = (int)value;
@@ -772,6 +798,8 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_GRID_MAX: *value = h->grid_max; return PGMG_OK;
         case PGMG_OPT_GS_VECTOR: *value = h->gs_vec; return PGMG_OK;
         case PGMG_OPT_INNER_DIGITS: *value = h->inner_digits; return PGMG_OK;
+        case PGMG_OPT_GS_ALTERNATE: *value = h->gs_alt; return PGMG_OK;
+        case PGMG_OPT_GS_PREFETCH: *value = h->gs_prefetch; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1066,7 +1094,8 @@ struct TuneKey {
 struct TuneVal {
     int gs_block, coarse_first, cluster_size, pdl;
     long long grid_max;
-    int gs_vec;
+    int gs_vec, gs_alt;
+    long long gs_prefetch;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1079,6 +1108,8 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->pdl = v.pdl != 0;
     h->grid_max = v.grid_max;
     h->gs_vec = v.gs_vec != 0;
+    h->gs_alt = v.gs_alt != 0;
+    h->gs_prefetch = v.gs_prefetch;
     drop_graphs(h);
 }
 
@@ -1141,7 +1172,8 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    TuneVal best{h->gs_block, h->coarse_first, h->cluster_size, h->pdl ? 1 : 0, h->grid_max, h->gs_vec ? 1 : 0, 0};
+    TuneVal best{h->gs_block, h->coarse_first,  h->cluster_size,   h->pdl ? 1 : 0,         h->grid_max,
+                 h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1155,6 +1187,20 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     };
     bool mc8 = h->dims.smoother == PGMG_SMOOTH_MC8;
     // Coordinate descent: one option at a time, each from the best so far.
+    if (st == PGMG_OK && mc8) {
+        TuneVal c = best;
+        c.gs_alt = !best.gs_alt;
+        st = trial(c);
+    }
+    if (st == PGMG_OK && mc8 && !h->prd) {
+        long long p0 = best.gs_prefetch;
+        for (long long pm : {0LL, 1LL << 18, 1LL << 22, 1LL << 26}) {
+            if (st != PGMG_OK || pm == p0) continue;
+            TuneVal c = best;
+            c.gs_prefetch = pm;
+            st = trial(c);
+        }
+    }
     if (st == PGMG_OK && mc8 && !h->prd) {
         TuneVal c = best;
         c.gs_vec = !best.gs_vec;

@@ -108,6 +108,11 @@ struct pgmg_handle {
     bool pdl = true;
     int gs_block = 256;  // threads per block of the colour sweep
     bool gs_vec = false;  // colour sweep with 16-byte vector loads (k_gs_colour_v)
+    bool gs_alt = true;   // colour passes alternate their traversal direction
+    // 8-colour levels of at most gs_prefetch points load their stencil before
+    // the launch dependency (k_gs_colour_pf); 0 = none.  On the largest
+    // levels the extra registers cost more occupancy than the overlap wins.
+    long long gs_prefetch = 1LL << 22;
     int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident

@@ -56,11 +56,17 @@ __device__ __forceinline__ void gs_colour_at(const LevelGeom& g, T* x, const T* 
 }
 
 // BS: threads per block (the autotuner picks 128, 256 or 512 per handle).
+// rev: blocks take the points from the top (last z planes) down.  Blocks
+// are scheduled in index order, so a pass with rev = 1 starts where the
+// previous pass ended and reads the solution planes that pass left in L2;
+// the points of one colour are independent, so the order changes no result.
 template <class T, bool EXACT, bool PRD = false, int BS = kBlock>
 __global__ void __launch_bounds__(BS) k_gs_colour(LevelGeom g, T* x, const T* __restrict__ r,
-                                                      const T* __restrict__ A, int col, int k2lo, int k2hi) {
+                                                      const T* __restrict__ A, int col, int k2lo, int k2hi,
+                                                      int rev) {
     pdl_enter();
-    long p = (long)k2lo * g.M2 * g.N2 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+    unsigned b = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    long p = (long)k2lo * g.M2 * g.N2 + b * (long)blockDim.x + threadIdx.x;
     if (p >= (long)k2hi * g.M2 * g.N2) return;
     gs_colour_at<T, PRD>(g, x, r, A, col, p);
 }
@@ -74,11 +80,12 @@ __global__ void __launch_bounds__(BS) k_gs_colour(LevelGeom g, T* x, const T* __
 // are aligned: colour-major planes are padded to multiples of 64 points).
 template <class T, int BS>
 __global__ void __launch_bounds__(BS) k_gs_colour_v(LevelGeom g, T* x, const T* __restrict__ r,
-                                                    const T* __restrict__ A, int col) {
+                                                    const T* __restrict__ A, int col, int rev) {
     constexpr int V = 16 / sizeof(T);
     pdl_enter();
     long nc = (long)g.M2 * g.N2 * g.O2;
-    long p0 = (blockIdx.x * (long)BS + threadIdx.x) * V;
+    unsigned b = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    long p0 = (b * (long)BS + threadIdx.x) * V;
     if (p0 >= nc) return;
     uint64_t ps = policy_evict_first(), pk = policy_evict_last();
     const long safe = g.xi(0, 0, 0);  // a point whose 27 neighbours exist (halo)
@@ -111,6 +118,46 @@ __global__ void __launch_bounds__(BS) k_gs_colour_v(LevelGeom g, T* x, const T* 
 #pragma unroll
     for (int v = 0; v < V; v++)
         if (ok[v]) st_keep(x + xc[v], mul_rn<T>(sub_rn<T>(rv[v], acc[v]), T(1) / d[v]), pk);
+}
+
+// The colour pass with the stencil prefetched before the launch dependency:
+// launched as a programmatic dependent launch, a block may start while the
+// previous kernel still runs.  Its 27 coefficients -- 90 % of the bytes,
+// written only at set-up -- are loaded first; only then does it wait for
+// the previous kernel and load the source and the neighbours' x, which that
+// kernel may have written.  Same arithmetic as gs_value.
+template <class T, int BS>
+__global__ void __launch_bounds__(BS) k_gs_colour_pf(LevelGeom g, T* x, const T* __restrict__ r,
+                                                     const T* __restrict__ A, int col, int rev) {
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    unsigned b = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    long p = b * (long)BS + threadIdx.x;
+    bool ok = p < nc;
+    int i = 0, j = 0, k = 0;
+    if (ok) {
+        int i2, j2, k2;
+        decode_colour(g, p, i2, j2, k2);
+        i = 2 * i2 + (col & 1); j = 2 * j2 + ((col >> 1) & 1); k = 2 * k2 + (col >> 2);
+        ok = i < g.m && j < g.n && k < g.o;
+    }
+    uint64_t ps = policy_evict_first(), pk = policy_evict_last();
+    T a[27];
+    if (ok) {
+        const T* Ap = A + (long)col * 27 * g.Nc + p;
+#pragma unroll
+        for (int q = 0; q < 27; q++) a[q] = ld_stream(Ap + q * g.Nc, ps);
+    }
+    pdl_enter();
+    if (!ok) return;
+    long xc = g.xi(i, j, k);
+    T rv = ld_stream(r + (long)col * g.Nc + p, ps);
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 27; q++) {
+        if (q == 13) continue;
+        acc = madd<true, T>(acc, a[q], ld_keep(x + xc + slot_off(g, q), pk));
+    }
+    st_keep(x + xc, mul_rn<T>(sub_rn<T>(rv, acc), T(1) / a[13]), pk);
 }
 
 // Hyperplane t = i + 2j + 4k of the lexicographic order.  Every neighbour of

@@ -97,3 +97,37 @@ def test_gs_vector_bitwise(mno, precision):
         A.v_cycle(0)
         B.v_cycle(0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_gs_alternate_bitwise(precision):
+    """Colour passes alternating their traversal direction give the same
+    iterates as passes that all run bottom up."""
+    mno = (65, 49, 33)
+    A = make(mno, precision)
+    B = make(mno, precision)
+    A.set_option(P.OPT_GS_ALTERNATE, 0)
+    B.set_option(P.OPT_GS_ALTERNATE, 1)
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+@pytest.mark.parametrize("pdl", [0, 1])
+def test_gs_prefetch_bitwise(precision, pdl):
+    """Colour passes that load their stencil before the launch dependency
+    give the same iterates as the default passes, with and without
+    programmatic dependent launches."""
+    mno = (97, 65, 49)
+    A = make(mno, precision)
+    B = make(mno, precision)
+    for G in (A, B):
+        G.set_option(P.OPT_PDL, pdl)
+    A.set_option(P.OPT_GS_PREFETCH, 0)
+    B.set_option(P.OPT_GS_PREFETCH, 1 << 30)
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
