@@ -300,7 +300,7 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     if (F.g.prd)
         LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T, true>, F.g, Cl.g, vf.res, vc.r, vc.x);
     else
-        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
+        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict_fast<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
     return wrap_level<T>(h, l);
 }
 
@@ -308,7 +308,7 @@ template <class T>
 pgmg_status interp_level(pgmg_handle* h, int l) {
     Level& F = h->L[l - 1];
     Level& Cl = h->L[l];
-    LAUNCH(nblk(F.g.npts), kBlock, k_interp<T>, F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
+    LAUNCH(nblk((long)F.g.M2 * F.g.N2 * F.g.O2), kBlock, k_interp_cube<T>, F.g, Cl.g, view<T>(F).x, view<T>(Cl).x);
     return wrap_level<T>(h, l - 1);
 }
 

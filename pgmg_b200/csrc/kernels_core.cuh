@@ -460,6 +460,48 @@ __global__ void __launch_bounds__(kBlock) k_restrict(LevelGeom gf, LevelGeom gc,
     restrict_at<T, PRD>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
+// Value of fine role `role` (bit 0 x, 1 y, 2 z: upper point of the cube on
+// that axis) of a cube with coarse corners v[0..7] (x fastest).  `full`: the
+// cube is not the last one on any non-periodic axis; xs/ys/zs: its upper
+// point on that axis snaps onto the next coarse point.
+template <class T>
+__device__ __forceinline__ T interp_val(int role, bool full, bool xs, bool ys, bool zs, const T (&v)[8]) {
+    const T h = T(0.5), qq = T(0.25), e = T(0.125);
+    T val;
+    if (full) {
+        switch (role) {
+            case 0: val = v[0]; break;
+            case 1: val = h * (v[0] + v[1]); break;
+            case 2: val = h * (v[0] + v[2]); break;
+            case 3: val = qq * (((v[0] + v[1]) + v[2]) + v[3]); break;
+            case 4: val = h * (v[0] + v[4]); break;
+            case 5: val = qq * ((v[0] + v[1]) + (v[4] + v[5])); break;
+            case 6: val = qq * (((v[0] + v[2]) + v[4]) + v[6]); break;
+            default: val = e * (((((((v[0] + v[1]) + v[2]) + v[3]) + (v[4] + v[5])) + v[6]) + v[7])); break;
+        }
+    } else {
+        switch (role) {
+            case 0: val = v[0]; break;
+            case 1: val = xs ? v[1] : h * (v[0] + v[1]); break;
+            case 2: val = ys ? v[2] : h * (v[0] + v[2]); break;
+            case 4: val = zs ? v[4] : h * (v[0] + v[4]); break;
+            case 5:
+                val = zs ? (xs ? v[5] : h * (v[4] + v[5])) : (xs ? h * (v[1] + v[5]) : qq * (((v[0] + v[1]) + v[4]) + v[5]));
+                break;
+            case 6:
+                val = zs ? (ys ? v[6] : h * (v[4] + v[6])) : (ys ? h * (v[2] + v[6]) : qq * (((v[0] + v[2]) + v[4]) + v[6]));
+                break;
+            default: {
+                T t2 = ys ? (xs ? v[3] : h * (v[2] + v[3])) : (xs ? h * (v[1] + v[3]) : qq * (((v[0] + v[1]) + v[2]) + v[3]));
+                if (role == 3) { val = t2; break; }
+                T t3 = ys ? (xs ? v[7] : h * (v[6] + v[7])) : (xs ? h * (v[5] + v[7]) : qq * (((v[4] + v[5]) + v[6]) + v[7]));
+                val = zs ? t3 : h * (t3 + t2);
+            }
+        }
+    }
+    return val;
+}
+
 // Interpolation with correction add (region.cc:576-593): each fine point
 // belongs to exactly one 2x2x2 cube (C = t>>1, role t&1 per axis) and gets
 // the value interpolate_full (:752-772) or interpolate_partial (:779-810)
@@ -476,43 +518,14 @@ __device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& 
     long sy = gc.mx, sz = gc.mx * gc.my;
     // Corners outside the coarse grid read the zero halo; the formulas never
     // use them for fine points that exist.
-    T v0 = xcv[b], v1 = xcv[b + 1], v2 = xcv[b + sy], v3 = xcv[b + sy + 1];
-    T v4 = xcv[b + sz], v5 = xcv[b + sz + 1], v6 = xcv[b + sz + sy], v7 = xcv[b + sz + sy + 1];
-    const T h = T(0.5), qq = T(0.25), e = T(0.125);
-    int role = dx | (dy << 1) | (dz << 2);
-    T val;
+    T v[8] = {xcv[b], xcv[b + 1], xcv[b + sy], xcv[b + sy + 1],
+              xcv[b + sz], xcv[b + sz + 1], xcv[b + sz + sy], xcv[b + sz + sy + 1]};
     // Periodic axes: every cube is full, its upper coarse corner at the last
     // cube being coarse 0's image in the halo.
     const bool qx = px(gf), qy = py(gf), qz = pz(gf);
     bool full = (qx || Cx < cube_last(gf.m)) && (qy || Cy < cube_last(gf.n)) && (qz || Cz < cube_last(gf.o));
-    if (full) {
-        switch (role) {
-            case 0: val = v0; break;
-            case 1: val = h * (v0 + v1); break;
-            case 2: val = h * (v0 + v2); break;
-            case 3: val = qq * (((v0 + v1) + v2) + v3); break;
-            case 4: val = h * (v0 + v4); break;
-            case 5: val = qq * ((v0 + v1) + (v4 + v5)); break;
-            case 6: val = qq * (((v0 + v2) + v4) + v6); break;
-            default: val = e * (((((((v0 + v1) + v2) + v3) + (v4 + v5)) + v6) + v7)); break;
-        }
-    } else {
-        bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
-        switch (role) {
-            case 0: val = v0; break;
-            case 1: val = xs ? v1 : h * (v0 + v1); break;
-            case 2: val = ys ? v2 : h * (v0 + v2); break;
-            case 4: val = zs ? v4 : h * (v0 + v4); break;
-            case 5: val = zs ? (xs ? v5 : h * (v4 + v5)) : (xs ? h * (v1 + v5) : qq * (((v0 + v1) + v4) + v5)); break;
-            case 6: val = zs ? (ys ? v6 : h * (v4 + v6)) : (ys ? h * (v2 + v6) : qq * (((v0 + v2) + v4) + v6)); break;
-            default: {
-                T t2 = ys ? (xs ? v3 : h * (v2 + v3)) : (xs ? h * (v1 + v3) : qq * (((v0 + v1) + v2) + v3));
-                if (role == 3) { val = t2; break; }
-                T t3 = ys ? (xs ? v7 : h * (v6 + v7)) : (xs ? h * (v5 + v7) : qq * (((v4 + v5) + v6) + v7));
-                val = zs ? t3 : h * (t3 + t2);
-            }
-        }
-    }
+    bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
+    T val = interp_val<T>(dx | (dy << 1) | (dz << 2), full, xs, ys, zs, v);
     long xf_i = gf.xi(i, j, k);
     xf[xf_i] = xf[xf_i] + val;
 }
@@ -522,6 +535,109 @@ __global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T
                                                    const T* __restrict__ xcv) {
     pdl_enter();
     interp_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// The same interpolation with one thread per cube: its 8 coarse corners are
+// loaded once and its (up to) 8 fine points updated, each with interp_at's
+// value.  Cubes are enumerated like colour points (M2 x N2 x O2 of the fine
+// level), so cube C covers fine 2C and 2C+1 (when < the axis size) on each
+// axis -- every fine point exactly once.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
+                                                        const T* __restrict__ xcv) {
+    pdl_enter();
+    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (p >= (long)gf.M2 * gf.N2 * gf.O2) return;
+    int Cx, Cy, Cz;
+    decode_colour(gf, p, Cx, Cy, Cz);
+    long b = gc.xi(Cx, Cy, Cz);
+    long sy = gc.mx, sz = gc.mx * gc.my;
+    T v[8] = {xcv[b], xcv[b + 1], xcv[b + sy], xcv[b + sy + 1],
+              xcv[b + sz], xcv[b + sz + 1], xcv[b + sz + sy], xcv[b + sz + sy + 1]};
+    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
+    bool full = (qx || Cx < cube_last(gf.m)) && (qy || Cy < cube_last(gf.n)) && (qz || Cz < cube_last(gf.o));
+    bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
+    int i0 = 2 * Cx, j0 = 2 * Cy, k0 = 2 * Cz;
+    long f0 = gf.xi(i0, j0, k0);
+    T old[8];
+#pragma unroll
+    for (int role = 0; role < 8; role++) {
+        int dx = role & 1, dy = (role >> 1) & 1, dz = role >> 2;
+        bool in = i0 + dx < gf.m && j0 + dy < gf.n && k0 + dz < gf.o;
+        old[role] = in ? xf[f0 + dx + gf.mx * (dy + gf.my * dz)] : T(0);
+    }
+#pragma unroll
+    for (int role = 0; role < 8; role++) {
+        int dx = role & 1, dy = (role >> 1) & 1, dz = role >> 2;
+        if (i0 + dx < gf.m && j0 + dy < gf.n && k0 + dz < gf.o)
+            xf[f0 + dx + gf.mx * (dy + gf.my * dz)] = old[role] + interp_val<T>(role, full, xs, ys, zs, v);
+    }
+}
+
+// One axis of a coarse point whose transfer is the interior one: both cubes
+// I-1 and I exist, have their upper point and are not snapped, so the fine
+// points 2I-1, 2I, 2I+1 transfer with weights 1/2, 1, 1/2.
+__device__ __forceinline__ bool inner_axis(int I, int ma) {
+    return I >= 1 && I <= cube_last(ma) && has_upper(I, ma) && !snapped(I, ma);
+}
+
+// Restriction of a non-periodic level.  Coarse points interior on all three
+// axes run restrict_at's loops with the weights known at compile time (the
+// same contributions in the same order, all 27 loads issued first); the
+// others take restrict_at itself.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
+                                                          T* __restrict__ rc, T* __restrict__ xc) {
+    pdl_enter();
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gc.npts) return;
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
+    if (!(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o))) {
+        restrict_at<T, false>(gf, gc, res, rc, xc, q);
+        return;
+    }
+    // Per axis: cube a (0: I-1, 1: I), role d -> fine offset 2a+d-2 from 2I,
+    // weight 0 (not visited), 1/2, 1, 1/2.
+    T rv[27];
+#pragma unroll
+    for (int az = 0; az < 2; az++)
+#pragma unroll
+        for (int ay = 0; ay < 2; ay++)
+#pragma unroll
+            for (int ax = 0; ax < 2; ax++)
+#pragma unroll
+                for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+                    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                        for (int dx = 0; dx < 2; dx++) {
+                            int oz = 2 * az + dz - 2, oy = 2 * ay + dy - 2, ox = 2 * ax + dx - 2;
+                            if (ox < -1 || oy < -1 || oz < -1) continue;
+                            rv[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)] = res[gf.ri(2 * I + ox, 2 * J + oy, 2 * K + oz)];
+                        }
+    T acc = T(0);
+#pragma unroll
+    for (int az = 0; az < 2; az++)
+#pragma unroll
+        for (int ay = 0; ay < 2; ay++)
+#pragma unroll
+            for (int ax = 0; ax < 2; ax++)
+#pragma unroll
+                for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+                    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                        for (int dx = 0; dx < 2; dx++) {
+                            int oz = 2 * az + dz - 2, oy = 2 * ay + dy - 2, ox = 2 * ax + dx - 2;
+                            if (ox < -1 || oy < -1 || oz < -1) continue;
+                            double wx = ox ? 0.5 : 1.0, wy = oy ? 0.5 : 1.0, wz = oz ? 0.5 : 1.0;
+                            double w = wx * wy * wz;
+                            T rd = (T)(0.125 * w) * rv[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
+                            acc = add_rn<T>(acc, rd);
+                        }
+    rc[gc.ri(I, J, K)] = acc;
+    xc[gc.xi(I, J, K)] = T(0);
 }
 
 // ---------------------------------------------------------------------------
