@@ -133,7 +133,7 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *   PGMG_OPT_CLUSTER_FIRST  first level run by the one-cluster coarse cycle
  *                           (default: the first level of <= 50000 points;
  *                           = number of levels disables it)
- *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 16, 8, or 0 (off)
+ *   PGMG_OPT_CLUSTER_SIZE   CTAs of that cluster: 1, 2, 4, 8, 16, or 0 (off)
  *   PGMG_OPT_SLAB_BUDGET    bytes of solution vector per z-slab of the 8-colour
  *                           sweep (default 0 = one slab).  This one
  *                           changes the update order, so results change at
@@ -156,6 +156,12 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           solution planes the previous one left in L2
  *                           (default); 0 = always bottom up.  No counterpart
  *                           in the reference.
+ *   PGMG_OPT_COARSE_SHARED  1 = the cluster coarse cycle sweeps a level with
+ *                           its x held in every CTA's shared memory (levels
+ *                           whose halo'd x takes at most 200 KiB), updates
+ *                           written to all CTAs through distributed shared
+ *                           memory (default); 0 = x read from L2.  Same
+ *                           results.  No counterpart in the reference.
  *   PGMG_OPT_GS_PREFETCH    8-colour levels of at most this many points load
  *                           each colour pass's stencil coefficients before
  *                           waiting for the previous kernel (with PGMG_OPT_PDL,
@@ -192,7 +198,8 @@ enum {
     PGMG_OPT_GS_VECTOR = 12,
     PGMG_OPT_INNER_DIGITS = 13,
     PGMG_OPT_GS_ALTERNATE = 14,
-    PGMG_OPT_GS_PREFETCH = 15
+    PGMG_OPT_GS_PREFETCH = 15,
+    PGMG_OPT_COARSE_SHARED = 16
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after

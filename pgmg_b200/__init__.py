@@ -35,6 +35,7 @@ OPT_GS_VECTOR = 12
 OPT_INNER_DIGITS = 13
 OPT_GS_ALTERNATE = 14
 OPT_GS_PREFETCH = 15
+OPT_COARSE_SHARED = 16
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",

@@ -374,6 +374,17 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     cfg.gridDim = dim3(h->cluster_size, 1, 1);
     cfg.blockDim = dim3(kClusterThreads, 1, 1);
     cfg.stream = h->stream;
+    if (h->coarse_shared) {
+        // Room for the largest x copy of a level the cluster sweeps (levels
+        // whose copy does not fit sweep from global memory).
+        long need = 0;
+        for (int l = h->coarse_first; l < h->nl; l++) {
+            // The colour-major x copy and the staged stencils, for levels where both fit.
+            long b = cm_copy(h->L[l].g, h->cluster_size).bytes((int)sizeof(T));
+            if (b <= kCoarseXsMax && b > need) need = b;
+        }
+        cfg.dynamicSmemBytes = (size_t)need;
+    }
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = h->cluster_size;
@@ -390,7 +401,7 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
     return PGMG_OK;
 }
 
-// Largest usable cluster (16, non-portable, else 8) for the coarse cycle.
+// Clusters of `size` CTAs of the coarse cycle that fit on the device at once (0: not launchable).
 template <class T>
 int probe_cluster(int size) {
     cudaLaunchConfig_t cfg = {};
@@ -655,6 +666,13 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
             break;
         }
     }
+    if (cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseXsMax) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseXsMax) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        h->coarse_shared = false;
+    }
     h->coarse_first = h->nl - 1;
     for (int l = 0; l < h->nl; l++)
         if (h->L[l].g.npts <= kClusterMax) { h->coarse_first = l; break; }
@@ -732,7 +750,8 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             h->coarse_first = (int)value;
             break;
         case PGMG_OPT_CLUSTER_SIZE:
-            if (value != 0 && value != 8 && value != 16) return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 8 or 16");
+            if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
+                return fail(h, PGMG_ERR_ARG, "cluster size must be 0, 1, 2, 4, 8 or 16");
             if (value && h->prd) return fail(h, PGMG_ERR_UNSUPPORTED, "periodic problems run without the cluster coarse cycle");
             if (value && (probe_cluster<double>((int)value) <= 0 || probe_cluster<float>((int)value) <= 0))
                 return fail(h, PGMG_ERR_UNSUPPORTED, "cluster of %lld CTAs not launchable", value);
@@ -749,6 +768,9 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             break;
         case PGMG_OPT_GS_ALTERNATE:
             h->gs_alt = value != 0;
+            break;
+        case PGMG_OPT_COARSE_SHARED:
+            h->coarse_shared = value != 0;
             break;
         case PGMG_OPT_GS_PREFETCH:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
@@ -800,6 +822,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_INNER_DIGITS: *value = h->inner_digits; return PGMG_OK;
         case PGMG_OPT_GS_ALTERNATE: *value = h->gs_alt; return PGMG_OK;
         case PGMG_OPT_GS_PREFETCH: *value = h->gs_prefetch; return PGMG_OK;
+        case PGMG_OPT_COARSE_SHARED: *value = h->coarse_shared; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1221,11 +1244,22 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
             c.coarse_first = l;
             st = trial(c);
         }
-        int other = best.cluster_size == 16 ? 8 : 16;
-        if (st == PGMG_OK && probe_cluster<double>(other) > 0 && probe_cluster<float>(other) > 0) {
+        int s0 = best.cluster_size;
+        for (int cs : {1, 2, 4, 8, 16}) {
+            if (st != PGMG_OK || cs == s0 || probe_cluster<double>(cs) <= 0 || probe_cluster<float>(cs) <= 0) continue;
             TuneVal c = best;
-            c.cluster_size = other;
+            c.cluster_size = cs;
             st = trial(c);
+        }
+        // A smaller cluster may prefer a lower first level: try its neighbours.
+        if (st == PGMG_OK && best.cluster_size != s0) {
+            int f1 = best.coarse_first;
+            for (int l : {f1 - 1, f1 + 1}) {
+                if (l < 0 || l > h->nl || (l < h->nl && h->L[l].g.npts > 6 * kClusterMax)) continue;
+                TuneVal c = best;
+                c.coarse_first = l;
+                if ((st = trial(c)) != PGMG_OK) break;
+            }
         }
     }
     if (st == PGMG_OK && mc8 && !h->prd && h->grid_blocks[0] > 0 && h->grid_blocks[1] > 0) {

@@ -19,6 +19,7 @@ constexpr long kLexBlockMax = 40000;  // levels up to this size sweep lexicograp
 constexpr long kMc8BlockMax = 10000;  // levels up to this size sweep 8 colours in one block
 constexpr long kClusterMax = 50000;   // levels up to this size run in the one-cluster coarse cycle
 constexpr int kClusterThreads = 512;
+constexpr int kCoarseXsMax = 200 * 1024;  // dynamic shared memory for a coarse level's x copy
 // Residual-check schedule (single solves and batches): check one cycle
 // before the predicted count when that cycle's predicted residual is within
 // kSlack of tol.  Mixed precision: the largest reduction asked of the FP32
@@ -113,6 +114,9 @@ struct pgmg_handle {
     // the launch dependency (k_gs_colour_pf); 0 = none.  On the largest
     // levels the extra registers cost more occupancy than the overlap wins.
     long long gs_prefetch = 1LL << 22;
+    // Coarse-cycle sweeps keep the level's x in each CTA's shared memory
+    // (levels whose halo'd x fits in kCoarseXsMax bytes).
+    bool coarse_shared = true;
     int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident

@@ -90,7 +90,7 @@ __device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T*
     const long xc0 = g.xi(i0, j0, k0), sy = g.mx, sz = g.mx * g.my;
     const int per = mode ? 16 : 8, total = sweeps * per;
     T a[27];
-    T rv = T(0);
+    T rv = T(0), ainv = T(1);
     auto colour_at = [&](int st) {
         int cc = st % per;
         return cc < 8 ? cc : 15 - cc;
@@ -104,6 +104,7 @@ __device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T*
 #pragma unroll
         for (int q = 0; q < 27; q++) a[q] = __ldg(Ap + q * g.Nc);
         rv = __ldcg(r + (long)col * g.Nc + tid);
+        ainv = T(1) / a[13];  // off the pass's critical path
     };
     if (total > 0) fetch(colour_at(0));
     for (int st = 0; st < total; st++) {
@@ -116,7 +117,7 @@ __device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T*
                 if (q == 13) continue;
                 acc = madd<true, T>(acc, a[q], __ldcg(x + xc + slot_off(g, q)));
             }
-            x[xc] = mul_rn<T>(sub_rn<T>(rv, acc), T(1) / a[13]);
+            x[xc] = mul_rn<T>(sub_rn<T>(rv, acc), ainv);
         }
         cl_arrive();
         if (st + 1 < total) fetch(colour_at(st + 1));
@@ -124,12 +125,143 @@ __device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T*
     }
 }
 
+// Distributed shared memory helpers: a CTA's shared-window address, the same
+// offset in the shared memory of CTA `rank` of the cluster, and a store there.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t cl_map(uint32_t a, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cl(uint32_t a, double v) {
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_cl(uint32_t a, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ unsigned dyn_smem_bytes() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+    return r;
+}
+
+// Shared-memory copy of a level for c_sweeps_shared: x in colour-major
+// order, each colour's (M2+2) x (N2+2) x (O2+2) sub-grid padded by one cube
+// on every side (zeros, like the halo), then the staged stencils.
+struct CmCopy {
+    int W, H;     // padded sub-grid row and plane extents: M2+2, N2+2
+    long Pn;      // padded points per colour
+    long chunk;   // colour points owned per CTA
+    long xelems;  // elements of the x copy (8*Pn, rounded up to even)
+    __host__ __device__ long bytes(int tsize) const { return (xelems + 8 * 28 * chunk) * tsize; }
+};
+__host__ __device__ inline CmCopy cm_copy(const LevelGeom& g, int csize) {
+    CmCopy c;
+    c.W = g.M2 + 2;
+    c.H = g.N2 + 2;
+    c.Pn = (long)c.W * c.H * (g.O2 + 2);
+    long nc = (long)g.M2 * g.N2 * g.O2;
+    c.chunk = (nc + csize - 1) / csize;
+    c.xelems = (8 * c.Pn + 1) & ~1L;
+    return c;
+}
+
+// c_sweeps_owned with the level held in shared memory.  Every CTA of the
+// cluster keeps a colour-major copy of x (copied in from global memory at
+// the start) and the coefficients, source and diagonal reciprocal of the
+// points it owns (as[colour][28][chunk]: slots 0..26 the stencil with slot 13
+// holding 1/diagonal, slot 27 the source).  Colour points are owned in
+// contiguous chunks, one per CTA.  A pass reads the neighbours from the
+// CTA's own copy and writes each new value into the copies of the CTAs that
+// own a point within reach of it (its neighbours lie within
+// +-(M2*N2 + M2 + 1) colour points), with coalesced st.shared::cluster
+// stores, ordered by the same cluster barriers: no pass waits for L2.  A
+// CTA's copy is current for the points its own points read.  At the end
+// each owner writes its points back to global memory.  Same arithmetic as
+// c_sweeps_owned.
+template <class T>
+__device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r, const T* A, int sweeps,
+                                             int mode, T* sm, int rank, int csize) {
+    const CmCopy cm = cm_copy(g, csize);
+    const long nc = (long)g.M2 * g.N2 * g.O2;
+    const int chunk = (int)cm.chunk, W = cm.W, H = cm.H, Pn = (int)cm.Pn;
+    long p = (long)rank * chunk + threadIdx.x;
+    bool have = (int)threadIdx.x < chunk && p < nc;
+    int i2 = 0, j2 = 0, k2 = 0;
+    if (have) decode_colour(g, p, i2, j2, k2);
+    const int pown = (i2 + 1) + W * ((j2 + 1) + H * (k2 + 1));
+    T* as = sm + cm.xelems;
+    __shared__ int offs[8 * 27];
+    // Copy in: padded entries and points outside the level stay zero.
+    for (long e = threadIdx.x; e < 8 * cm.Pn; e += blockDim.x) {
+        int c = (int)(e / Pn), P = (int)(e - (long)c * Pn);
+        int pk = P / (W * H), pr = P - pk * W * H, pj = pr / W, pi = pr - pj * W;
+        int i = 2 * (pi - 1) + (c & 1), j = 2 * (pj - 1) + ((c >> 1) & 1), k = 2 * (pk - 1) + (c >> 2);
+        bool in = pi >= 1 && pj >= 1 && pk >= 1 && i < g.m && j < g.n && k < g.o;
+        sm[e] = in ? __ldcg(x + g.xi(i, j, k)) : T(0);
+    }
+    // Offset of neighbour slot q of a colour-c point from its own cube's index.
+    for (int e = threadIdx.x; e < 8 * 27; e += blockDim.x) {
+        int c = e / 27, q = e - c * 27;
+        int ti = (c & 1) + q % 3 - 1, tj = ((c >> 1) & 1) + (q / 3) % 3 - 1, tk = (c >> 2) + q / 9 - 1;
+        int cn = (ti & 1) | ((tj & 1) << 1) | ((tk & 1) << 2);
+        offs[e] = cn * Pn + (ti >> 1) + W * ((tj >> 1) + H * (tk >> 1));
+    }
+    auto valid = [&](int col) {
+        return have && 2 * i2 + (col & 1) < g.m && 2 * j2 + ((col >> 1) & 1) < g.n && 2 * k2 + (col >> 2) < g.o;
+    };
+    for (int col = 0; col < 8; col++) {
+        // Thread t stages its own points and reads them back itself.
+        if (!valid(col)) continue;
+        const T* Ap = A + (long)col * 27 * g.Nc + p;
+        T* sp = as + (long)col * 28 * chunk + threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < 27; q++) sp[q * chunk] = q == 13 ? T(1) / __ldg(Ap + 13 * g.Nc) : __ldg(Ap + q * g.Nc);
+        sp[27 * chunk] = __ldcg(r + (long)col * g.Nc + p);
+    }
+    // CTAs whose points read this CTA's points.
+    const long span = (long)g.M2 * g.N2 + g.M2 + 1;
+    long plo = (long)rank * chunk - span, phi = (long)(rank + 1) * chunk - 1 + span;
+    const int dlo = plo < 0 ? 0 : (int)(plo / chunk);
+    const int dhi = (int)(phi / chunk) < csize - 1 ? (int)(phi / chunk) : csize - 1;
+    const uint32_t base = smem_u32(sm);
+    const int per = mode ? 16 : 8, total = sweeps * per;
+    // Every copy (and the offset table) is complete before any CTA writes
+    // into another's.
+    cluster_sync();
+    for (int st = 0; st < total; st++) {
+        int cc = st % per;
+        int col = cc < 8 ? cc : 15 - cc;
+        if (valid(col)) {
+            const T* sp = as + col * 28 * chunk + threadIdx.x;
+            const int* oq = offs + col * 27;
+            T acc = T(0);
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                if (q == 13) continue;
+                acc = madd<true, T>(acc, sp[q * chunk], sm[pown + oq[q]]);
+            }
+            T v = mul_rn<T>(sub_rn<T>(sp[27 * chunk], acc), sp[13 * chunk]);
+            uint32_t off = base + (uint32_t)(col * Pn + pown) * (uint32_t)sizeof(T);
+            for (int d = dlo; d <= dhi; d++) st_cl(cl_map(off, (uint32_t)d), v);
+        }
+        cluster_sync();
+    }
+    for (int col = 0; col < 8; col++)
+        if (valid(col))
+            x[g.xi(2 * i2 + (col & 1), 2 * j2 + ((col >> 1) & 1), 2 * k2 + (col >> 2))] = sm[col * Pn + pown];
+    cluster_sync();
+}
+
 template <class T>
 __device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, const T* A, int sweeps, int mode,
-                                         long long budget, int tid, int nth) {
+                                         long long budget, int tid, int nth, T* xs, int rank, int csize) {
     int S = slab_count(g, (int)sizeof(T), budget);
     if (S == 1 && (long)g.M2 * g.N2 * g.O2 <= nth) {
-        c_sweeps_owned<T>(g, x, r, A, sweeps, mode, tid);
+        if (xs && cm_copy(g, csize).bytes((int)sizeof(T)) <= (long)dyn_smem_bytes())
+            c_sweeps_shared<T>(g, x, r, A, sweeps, mode, xs, rank, csize);
+        else
+            c_sweeps_owned<T>(g, x, r, A, sweeps, mode, tid);
         return;
     }
     for (int s = 0; s < sweeps; s++)
@@ -311,10 +443,15 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(const CoarsePlan<T>* __res
     if (active && !active[slot]) return;
     const CoarsePlan<T>& P = plans[slot];
     int nth = csize * blockDim.x;
-    int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+    int rank = (int)cl.block_rank();
+    int tid = rank * blockDim.x + threadIdx.x;
     int nl = P.nl;
+    // Shared copy of a level's x for the sweeps (when launched with dynamic
+    // shared memory; every CTA of the cluster has the same amount).
+    extern __shared__ __align__(16) unsigned char c_dyn[];
+    T* xs = dyn_smem_bytes() > 0 ? reinterpret_cast<T*>(c_dyn) : nullptr;
     for (int l = P.first; l < nl - 1; l++) {
-        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.v_down + l, mode, P.slab_budget, tid, nth);
+        c_sweeps<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.v_down + l, mode, P.slab_budget, tid, nth, xs, rank, csize);
         c_residual<T>(P.g[l], P.x[l], P.r[l], P.A[l], P.res[l], tid, nth);
         cluster_sync();
         c_restrict<T>(P.g[l], P.g[l + 1], P.res[l], P.r[l + 1], P.x[l + 1], tid, nth);
@@ -326,12 +463,13 @@ __global__ void __launch_bounds__(512) k_coarse_cycle(const CoarsePlan<T>* __res
         c_lu_apply<T>(P.g[lb], P.Minv, P.r[lb], P.x[lb], tid, nth, sh_src);
         cluster_sync();
     } else {
-        c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, P.slab_budget, tid, nth);
+        c_sweeps<T>(P.g[lb], P.x[lb], P.r[lb], P.A[lb], 24, 0, P.slab_budget, tid, nth, xs, rank, csize);
     }
     for (int l = lb; l > P.first; l--) {
         c_interp<T>(P.g[l - 1], P.g[l], P.x[l - 1], P.x[l], tid, nth);
         cluster_sync();
-        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], P.v_up + l - 1, mode, P.slab_budget, tid, nth);
+        c_sweeps<T>(P.g[l - 1], P.x[l - 1], P.r[l - 1], P.A[l - 1], P.v_up + l - 1, mode, P.slab_budget, tid, nth, xs,
+                    rank, csize);
     }
 }
 

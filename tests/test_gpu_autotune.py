@@ -28,7 +28,7 @@ def test_autotune_changes_no_result(mno, precision):
     B = make(mno, precision)
     t = B.autotune()
     assert t["gs_block"] in (128, 256, 512) and t["pdl"] in (0, 1) and t["vcycle_ms"] > 0
-    assert 0 <= t["cluster_first"] <= B.nlevels and t["cluster_size"] in (8, 16)
+    assert 0 <= t["cluster_first"] <= B.nlevels and t["cluster_size"] in (1, 2, 4, 8, 16)
     B.clear_x(0)
     B.solve(1e-10, 100, 1)
     assert np.array_equal(B.get_x(0), xa)
@@ -130,4 +130,24 @@ def test_gs_prefetch_bitwise(precision, pdl):
     for _ in range(2):
         A.v_cycle(0)
         B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+@pytest.mark.parametrize("mno,first", [((65, 65, 65), 2), ((97, 81, 49), 2), ((129, 129, 129), 3)])
+def test_coarse_shared_bitwise(precision, mno, first):
+    """The cluster coarse cycle sweeping from a shared-memory copy of each
+    level's x gives the same iterates as sweeping from global memory."""
+    A = make(mno, precision)
+    B = make(mno, precision)
+    for G in (A, B):
+        G.set_option(P.OPT_CLUSTER_FIRST, first)
+    A.set_option(P.OPT_COARSE_SHARED, 0)
+    B.set_option(P.OPT_COARSE_SHARED, 1)
+    for _ in range(3):
+        A.v_cycle(0)
+        B.v_cycle(0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+    for G in (A, B):
+        c, rr = G.solve(1e-10, 60, 0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
