@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON file of autotuner choices: a shape found there is not re-tuned (so that the same "
+                         "command run under a profiler uses the options a plain run chose)")
     ap.add_argument("--workload", default="solve257",
                     choices=["solve257", "small65", "large513", "batch96", "serve"],
                     help="solve257 is the benchmark line; the others measure the other configurations")
@@ -268,7 +271,7 @@ def run_ours(a):
         r = G.get_field(0, P.FIELD_R)
     # Result-neutral execution options chosen by the library's autotuner
     # (before any timed region).
-    tuning = G.autotune()
+    tuning = G.autotune(cache=a.tune_cache)
 
     def solve_once(H):
         H.clear_x(0)
@@ -339,7 +342,7 @@ def run_ours(a):
         Gm = P.Multigrid(m, m, m, precision=P.MIXED, coarse=P.COARSE_LU, smoother=smoother, device=local)
         Gm.set_stream(stream.cuda_stream)
         setup(Gm)
-        mixed_tuning = Gm.autotune()
+        mixed_tuning = Gm.autotune(cache=a.tune_cache)
         for _ in range(a.warmup):
             mc, mr = solve_once(Gm)
         torch.cuda.synchronize()

@@ -14,6 +14,7 @@ The host problem generators (``problem_kappa``, ``problem_q1``,
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 
 import numpy as np
@@ -274,17 +275,44 @@ class Multigrid:
         self._ck(lib().pgmg_dev_get_option(self._h, key, C.byref(v)), "get_option")
         return v.value
 
-    def autotune(self, reps: int = 3) -> dict:
+    # Result-neutral execution options the autotuner chooses among.
+    TUNED_OPTIONS = {"gs_block": OPT_GS_BLOCK, "cluster_size": OPT_CLUSTER_SIZE, "cluster_first": OPT_CLUSTER_FIRST,
+                     "pdl": OPT_PDL, "grid_max": OPT_GRID_MAX, "gs_vector": OPT_GS_VECTOR,
+                     "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH}
+
+    def autotune(self, reps: int = 3, cache: str = None) -> dict:
         """Times V-cycles under the result-neutral execution options and keeps
         the fastest (pgmg_dev_autotune); returns the chosen options and the
-        V-cycle time in ms."""
+        V-cycle time in ms.
+
+        ``cache``: a JSON file of earlier choices, keyed by grid shape,
+        precision, smoother and coarse solve.  A shape found there gets the
+        stored options without timing (``"cached": True`` in the result);
+        otherwise the choice made here is added to the file.  This lets a
+        second process -- for instance the same program run under a
+        profiler, where timings mean nothing -- use the options a plain run
+        chose."""
+        key = "%dx%dx%d/p%d/s%d/c%d" % (self.m, self.n, self.o, self.precision, self.smoother, self.coarse)
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                known = json.load(f)
+            if key in known:
+                for name, opt in self.TUNED_OPTIONS.items():
+                    self.set_option(opt, int(known[key][name]))
+                return dict(known[key], cached=True)
         ms = C.c_double()
         self._ck(lib().pgmg_dev_autotune(self._h, int(reps), C.byref(ms)), "autotune")
-        return {"gs_block": self.get_option(OPT_GS_BLOCK), "cluster_first": self.get_option(OPT_CLUSTER_FIRST),
-                "cluster_size": self.get_option(OPT_CLUSTER_SIZE), "pdl": self.get_option(OPT_PDL),
-                "grid_max": self.get_option(OPT_GRID_MAX), "gs_vector": self.get_option(OPT_GS_VECTOR),
-                "gs_alternate": self.get_option(OPT_GS_ALTERNATE), "gs_prefetch": self.get_option(OPT_GS_PREFETCH),
-                "vcycle_ms": ms.value}
+        out = {name: self.get_option(opt) for name, opt in self.TUNED_OPTIONS.items()}
+        out["vcycle_ms"] = ms.value
+        if cache:
+            known = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    known = json.load(f)
+            known[key] = out
+            with open(cache, "w") as f:
+                json.dump(known, f, indent=1)
+        return out
 
     def set_smoother(self, smoother: int):
         self._ck(lib().pgmg_dev_set_smoother(self._h, smoother), "set_smoother")

@@ -151,3 +151,20 @@ def test_coarse_shared_bitwise(precision, mno, first):
     for G in (A, B):
         c, rr = G.solve(1e-10, 60, 0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+def test_autotune_cache_file(tmp_path):
+    """A shape in the tuning cache gets the stored options without timing."""
+    cache = str(tmp_path / "tune.json")
+    A = make((65, 49, 33), P.FP64)
+    t = A.autotune(cache=cache)
+    assert "cached" not in t
+    B = make((65, 49, 33), P.FP64)
+    B.set_option(P.OPT_GS_BLOCK, 512 if t["gs_block"] != 512 else 128)
+    t2 = B.autotune(cache=cache)
+    assert t2["cached"] is True
+    for name, opt in P.Multigrid.TUNED_OPTIONS.items():
+        assert B.get_option(opt) == t[name]
+    # Another precision is a different entry.
+    C = make((65, 49, 33), P.MIXED)
+    assert "cached" not in C.autotune(cache=cache)
