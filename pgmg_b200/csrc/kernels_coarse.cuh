@@ -145,111 +145,93 @@ __device__ __forceinline__ unsigned dyn_smem_bytes() {
     return r;
 }
 
-// Shared-memory copy of a level for c_sweeps_shared: x in colour-major
-// order, each colour's (M2+2) x (N2+2) x (O2+2) sub-grid padded by one cube
-// on every side (zeros, like the halo), then the staged stencils.
+// Shared-memory copy of a level for c_sweeps_shared: the halo'd x array in
+// its global (natural) layout, then the staged stencils.
 struct CmCopy {
-    int W, H;     // padded sub-grid row and plane extents: M2+2, N2+2
-    long Pn;      // padded points per colour
+    long nc;      // colour points per colour
     long chunk;   // colour points owned per CTA
-    long xelems;  // elements of the x copy (8*Pn, rounded up to even)
+    long xelems;  // elements of the x copy (the halo'd array, rounded up to even)
     __host__ __device__ long bytes(int tsize) const { return (xelems + 8 * 28 * chunk) * tsize; }
 };
 __host__ __device__ inline CmCopy cm_copy(const LevelGeom& g, int csize) {
     CmCopy c;
-    c.W = g.M2 + 2;
-    c.H = g.N2 + 2;
-    c.Pn = (long)c.W * c.H * (g.O2 + 2);
-    long nc = (long)g.M2 * g.N2 * g.O2;
-    c.chunk = (nc + csize - 1) / csize;
-    c.xelems = (8 * c.Pn + 1) & ~1L;
+    c.nc = (long)g.M2 * g.N2 * g.O2;
+    c.chunk = (c.nc + csize - 1) / csize;
+    c.xelems = (g.xsize() + 1) & ~1L;
     return c;
 }
 
 // c_sweeps_owned with the level held in shared memory.  Every CTA of the
-// cluster keeps a colour-major copy of x (copied in from global memory at
-// the start) and the coefficients, source and diagonal reciprocal of the
+// cluster keeps a copy of the halo'd x array (copied in from global memory
+// at the start) and the coefficients, source and diagonal reciprocal of the
 // points it owns (as[colour][28][chunk]: slots 0..26 the stencil with slot 13
 // holding 1/diagonal, slot 27 the source).  Colour points are owned in
 // contiguous chunks, one per CTA.  A pass reads the neighbours from the
-// CTA's own copy and writes each new value into the copies of the CTAs that
-// own a point within reach of it (its neighbours lie within
-// +-(M2*N2 + M2 + 1) colour points), with coalesced st.shared::cluster
-// stores, ordered by the same cluster barriers: no pass waits for L2.  A
-// CTA's copy is current for the points its own points read.  At the end
-// each owner writes its points back to global memory.  Same arithmetic as
-// c_sweeps_owned.
+// CTA's own copy (a neighbour's offset is the same for every colour, so a
+// read is one add and one load) and writes each new value into the copies of
+// the CTAs that own a point within reach of it (its neighbours lie within
+// +-(M2*N2 + M2 + 1) colour points) with st.shared::cluster stores, ordered
+// by the same cluster barriers: no pass waits for L2.  A CTA's copy is
+// current for the points its own points read.  At the end each owner writes
+// its points back to global memory.  Same arithmetic as c_sweeps_owned.
 template <class T>
 __device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r, const T* A, int sweeps,
                                              int mode, T* sm, int rank, int csize) {
     const CmCopy cm = cm_copy(g, csize);
-    const long nc = (long)g.M2 * g.N2 * g.O2;
-    const int chunk = (int)cm.chunk, W = cm.W, H = cm.H, Pn = (int)cm.Pn;
-    long p = (long)rank * chunk + threadIdx.x;
-    bool have = (int)threadIdx.x < chunk && p < nc;
+    const int nc = (int)cm.nc, chunk = (int)cm.chunk;
+    const int p = rank * chunk + (int)threadIdx.x;
+    const bool have = (int)threadIdx.x < chunk && p < nc;
     int i2 = 0, j2 = 0, k2 = 0;
     if (have) decode_colour(g, p, i2, j2, k2);
-    const int pown = (i2 + 1) + W * ((j2 + 1) + H * (k2 + 1));
+    // Shared-memory indexes fit in 32 bits (the copies are at most kCoarseXsMax bytes).
+    const int mxi = (int)g.mx, szi = (int)(g.mx * g.my);
+    const int xc0 = (int)g.xi(2 * i2, 2 * j2, 2 * k2);
     T* as = sm + cm.xelems;
-    __shared__ int offs[8 * 27];
-    // Copy in: padded entries and points outside the level stay zero.
-    for (long e = threadIdx.x; e < 8 * cm.Pn; e += blockDim.x) {
-        int c = (int)(e / Pn), P = (int)(e - (long)c * Pn);
-        int pk = P / (W * H), pr = P - pk * W * H, pj = pr / W, pi = pr - pj * W;
-        int i = 2 * (pi - 1) + (c & 1), j = 2 * (pj - 1) + ((c >> 1) & 1), k = 2 * (pk - 1) + (c >> 2);
-        bool in = pi >= 1 && pj >= 1 && pk >= 1 && i < g.m && j < g.n && k < g.o;
-        sm[e] = in ? __ldcg(x + g.xi(i, j, k)) : T(0);
-    }
-    // Offset of neighbour slot q of a colour-c point from its own cube's index.
-    for (int e = threadIdx.x; e < 8 * 27; e += blockDim.x) {
-        int c = e / 27, q = e - c * 27;
-        int ti = (c & 1) + q % 3 - 1, tj = ((c >> 1) & 1) + (q / 3) % 3 - 1, tk = (c >> 2) + q / 9 - 1;
-        int cn = (ti & 1) | ((tj & 1) << 1) | ((tk & 1) << 2);
-        offs[e] = cn * Pn + (ti >> 1) + W * ((tj >> 1) + H * (tk >> 1));
-    }
+    const int xn = (int)g.xsize();
+    for (int e = threadIdx.x; e < xn; e += blockDim.x) sm[e] = __ldcg(x + e);
     auto valid = [&](int col) {
         return have && 2 * i2 + (col & 1) < g.m && 2 * j2 + ((col >> 1) & 1) < g.n && 2 * k2 + (col >> 2) < g.o;
     };
+    auto at = [&](int col) { return xc0 + (col & 1) + ((col >> 1) & 1) * mxi + (col >> 2) * szi; };
     for (int col = 0; col < 8; col++) {
         // Thread t stages its own points and reads them back itself.
         if (!valid(col)) continue;
         const T* Ap = A + (long)col * 27 * g.Nc + p;
-        T* sp = as + (long)col * 28 * chunk + threadIdx.x;
+        T* sp = as + col * 28 * chunk + threadIdx.x;
 #pragma unroll
         for (int q = 0; q < 27; q++) sp[q * chunk] = q == 13 ? T(1) / __ldg(Ap + 13 * g.Nc) : __ldg(Ap + q * g.Nc);
         sp[27 * chunk] = __ldcg(r + (long)col * g.Nc + p);
     }
     // CTAs whose points read this CTA's points.
-    const long span = (long)g.M2 * g.N2 + g.M2 + 1;
-    long plo = (long)rank * chunk - span, phi = (long)(rank + 1) * chunk - 1 + span;
-    const int dlo = plo < 0 ? 0 : (int)(plo / chunk);
-    const int dhi = (int)(phi / chunk) < csize - 1 ? (int)(phi / chunk) : csize - 1;
+    const int span = g.M2 * g.N2 + g.M2 + 1;
+    const int plo = rank * chunk - span, phi = (rank + 1) * chunk - 1 + span;
+    const int dlo = plo < 0 ? 0 : plo / chunk;
+    const int dhi = phi / chunk < csize - 1 ? phi / chunk : csize - 1;
     const uint32_t base = smem_u32(sm);
     const int per = mode ? 16 : 8, total = sweeps * per;
-    // Every copy (and the offset table) is complete before any CTA writes
-    // into another's.
+    // Every copy is complete before any CTA writes into another's.
     cluster_sync();
     for (int st = 0; st < total; st++) {
         int cc = st % per;
         int col = cc < 8 ? cc : 15 - cc;
         if (valid(col)) {
             const T* sp = as + col * 28 * chunk + threadIdx.x;
-            const int* oq = offs + col * 27;
+            const int xc = at(col);
+            const T* xp = sm + xc;
             T acc = T(0);
 #pragma unroll
             for (int q = 0; q < 27; q++) {
                 if (q == 13) continue;
-                acc = madd<true, T>(acc, sp[q * chunk], sm[pown + oq[q]]);
+                acc = madd<true, T>(acc, sp[q * chunk], xp[(q % 3 - 1) + mxi * ((q / 3) % 3 - 1) + szi * (q / 9 - 1)]);
             }
             T v = mul_rn<T>(sub_rn<T>(sp[27 * chunk], acc), sp[13 * chunk]);
-            uint32_t off = base + (uint32_t)(col * Pn + pown) * (uint32_t)sizeof(T);
+            uint32_t off = base + (uint32_t)xc * (uint32_t)sizeof(T);
             for (int d = dlo; d <= dhi; d++) st_cl(cl_map(off, (uint32_t)d), v);
         }
         cluster_sync();
     }
     for (int col = 0; col < 8; col++)
-        if (valid(col))
-            x[g.xi(2 * i2 + (col & 1), 2 * j2 + ((col >> 1) & 1), 2 * k2 + (col >> 2))] = sm[col * Pn + pown];
+        if (valid(col)) x[at(col)] = sm[at(col)];
     cluster_sync();
 }
 
