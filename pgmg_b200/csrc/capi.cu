@@ -492,14 +492,46 @@ pgmg_status run_vcycle(pgmg_handle* h, int mode, int smoother) {
     return PGMG_OK;
 }
 
+// A residual check's norms: call check_begin before launching the kernel
+// that writes the partial sums, then reduce_and_read, which leaves the two
+// norms in h->norm_host.  With the pinned pair the reduction writes them to
+// host memory directly, and the host waits in two steps: a blocking wait on
+// the event recorded before the residual kernel (the thread wakes while that
+// kernel still runs), then polling of the event after the reduction -- so
+// the norms are read within microseconds of being written, not a thread
+// wake-up later.
+constexpr long kNormPolls = 1L << 20;  // then a blocking wait
+
+pgmg_status check_begin(pgmg_handle* h) {
+    if (h->norm_pin) CK(cudaEventRecord(h->ev_pre, h->stream));
+    return PGMG_OK;
+}
+
+pgmg_status reduce_and_read(pgmg_handle* h, long nb) {
+    if (!h->norm_pin) {
+        LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
+        CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return PGMG_OK;
+    }
+    LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_pin);
+    CK(cudaEventRecord(h->ev_post, h->stream));
+    CK(cudaEventSynchronize(h->ev_pre));
+    cudaError_t e = cudaErrorNotReady;
+    for (long i = 0; i < kNormPolls && e == cudaErrorNotReady; i++) e = cudaEventQuery(h->ev_post);
+    if (e == cudaErrorNotReady) e = cudaEventSynchronize(h->ev_post);
+    CK(e);
+    h->norm_host[0] = h->norm_pin[0];
+    h->norm_host[1] = h->norm_pin[1];
+    return PGMG_OK;
+}
+
 // Norms of a level (FP64 data) into h->norm_host; synchronises.
 pgmg_status norms64(pgmg_handle* h, int l, double* res2, double* rhs2) {
     Level& L = h->L[l];
+    TRY(check_begin(h));
     TRY(residual_level<double>(h, l, nullptr, h->partials));
-    long nb = nblk((long)L.g.M2 * L.g.N2 * L.g.O2) * 8;
-    LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
-    CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    TRY(reduce_and_read(h, nblk((long)L.g.M2 * L.g.N2 * L.g.O2) * 8));
     if (res2) *res2 = h->norm_host[0];
     if (rhs2) *rhs2 = h->norm_host[1];
     return PGMG_OK;
@@ -512,12 +544,12 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
     Level& L0 = h->L[0];
     const LevelGeom& g = L0.g;
     dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
-    LAUNCH(grid, kBlock, k_residual<double, float, true>, g, L0.x64, L0.r64, L0.A64, L0.r32, h->partials);
+    if (res2 || rhs2) TRY(check_begin(h));
+    LAUNCH(grid, kBlock, k_residual<double, float, true>, g, L0.x64, L0.r64, L0.A64, L0.r32,
+           (res2 || rhs2) ? h->partials : nullptr);
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
-    LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
     if (res2 || rhs2) {
-        CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        TRY(reduce_and_read(h, nb));
         if (res2) *res2 = h->norm_host[0];
         if (rhs2) *rhs2 = h->norm_host[1];
     }
@@ -660,6 +692,13 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
         return PGMG_ERR_CUDA;
     }
     h->stream = h->own;
+    if (cudaMallocHost(&h->norm_pin, 2 * sizeof(double)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_pre, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_post, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (h->norm_pin) cudaFreeHost(h->norm_pin);
+        h->norm_pin = nullptr;  // checks fall back to a copy and a stream synchronisation
+    }
     for (int size : {16, 8}) {
         if (probe_cluster<double>(size) > 0 && probe_cluster<float>(size) > 0) {
             h->cluster_size = size;
@@ -713,6 +752,9 @@ pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
+    if (h->norm_pin) cudaFreeHost(h->norm_pin);
+    if (h->ev_pre) cudaEventDestroy(h->ev_pre);
+    if (h->ev_post) cudaEventDestroy(h->ev_post);
     if (h->arena.base && h->own_arena) cudaFree(h->arena.base);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
@@ -1422,6 +1464,7 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
         // (it is the next correction's source), so it checks every step too.
         bool check = mixed || nc >= next_check || nc >= max_cycles;
         bool zero = nc == 0 && h->x0_zero;  // residual = source: no stencil pass needed
+        if (check) TRY(check_begin(h));
         if (zero) {
             if (mixed || check) {
                 LAUNCH(grid, kBlock, k_source<double, float>, g, L0.r64, mixed ? L0.r32 : nullptr, h->partials);
@@ -1436,9 +1479,7 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
                                                                                h->partials);
         }
         if (check) {
-            LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
-            CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
+            TRY(reduce_and_read(h, nb));
             res2 = h->norm_host[0];
             rhs2 = h->norm_host[1];
             rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);

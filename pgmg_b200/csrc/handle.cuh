@@ -94,6 +94,12 @@ struct pgmg_handle {
     double* partials = nullptr;
     double* norm_dev = nullptr;
     double norm_host[2] = {0, 0};
+    // Residual checks: the reduction writes the two norms straight into this
+    // pinned host pair (null if it could not be had: then they are copied
+    // from norm_dev); ev_pre is recorded before the check's residual kernel,
+    // ev_post after the reduction.
+    double* norm_pin = nullptr;
+    cudaEvent_t ev_pre = nullptr, ev_post = nullptr;
     bool own_arena = true;         // false: memory given by the caller
     // mg_guide state (multigrid.hh:34-118)
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;
