@@ -560,6 +560,59 @@ def run_large513(a):
     print(json.dumps(out))
 
 
+def _ref_problem_worker(job):
+    """One problem of the batch or serving CPU baseline, in a host process of
+    its own: the problem built with the host generators (the same arrays the
+    device generators give), the reference's set-up, then its V-cycles to tol
+    for each right-hand side.  Returns (set-up s, [solve s per RHS], cycles)."""
+    (m, n, o), sigma, field_seed, rhs_seeds, tol = job
+    import pgmg_b200 as P
+    from oracle.pyoracle import Reference
+    kap = P.problem_kappa(m, n, o, sigma, field_seed, 8.0)
+    coef, S = P.problem_q1(m, n, o, kap)
+    del kap
+    t0 = time.perf_counter()
+    R = Reference(m, n, o, S, coef, P.problem_rhs(m, n, o, rhs_seeds[0]))
+    setup = time.perf_counter() - t0
+    solves, cycles = [], []
+    for k, rs in enumerate(rhs_seeds):
+        if k:
+            R.set_r(0, P.problem_rhs(m, n, o, rs))
+        R.set_x(0, np.zeros(m * n * o))
+        t0 = time.perf_counter()
+        c, _ = reference_cycles(R, tol)
+        solves.append(time.perf_counter() - t0)
+        cycles.append(c)
+    return setup, solves, cycles
+
+
+def cpu_pool_baseline(jobs, with_setup, sample):
+    """The reference on the host cores: independent single-process solves,
+    one per core at a time (a spawn-started pool: no process forks after the
+    GPU is in use), throughput summed over the wall time of the sample."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    from oracle.pyoracle import ref_available
+    if not ref_available() or not jobs:
+        return None
+    cores = max(1, min(os.cpu_count() or 1, len(jobs), 16))
+    t0 = time.perf_counter()
+    # (A worker that dies breaks the pool and raises here, instead of being
+    # re-spawned.)
+    with ProcessPoolExecutor(cores, mp_context=mp.get_context("spawn")) as pool:
+        res = list(pool.map(_ref_problem_worker, jobs))
+    wall = time.perf_counter() - t0
+    nsol = sum(len(j[3]) for j in jobs)
+    busy = sum((st if with_setup else 0.0) + sum(sv) for st, sv, _ in res)
+    # Throughput of `cores` processes working through the sample: the work
+    # each would do back to back, summed, over the busy time per core.
+    return {"value": nsol / (busy / cores), "unit": "solves/s", "cores": cores, "kind": "reference",
+            "sample": sample + f"; {nsol} solves, {busy:.1f} s of reference time "
+                      f"({'set-up and ' if with_setup else ''}solves), {wall:.1f} s wall on {cores} processes",
+            "cycles_min_max": [min(min(c) for _, _, c in res), max(max(c) for _, _, c in res)]}
+
+
 def run_batch96(a):
     """Config 4: 96 independent problems, dims per axis from {33,65,129},
     sigma uniform in [0.5,2], mixed precision to 1e-10, one launch per level
@@ -607,6 +660,19 @@ def run_batch96(a):
     t_seq, _ = timed(st, seq, 1)
     alg = sum(int(c) * ir_step_bytes(*s) for c, s in zip(cyc[:nprob], shapes))
     peak, kind = measured_peak_hbm()
+    cpu = None
+    if not a.no_cpu_baseline:
+        # A bounded sample: the first problems of the batch up to about 3
+        # million points per host process.
+        budget, jobs, pts = 3e6 * max(1, min(os.cpu_count() or 1, 16)), [], 0
+        for p, (shape, sg) in enumerate(zip(shapes, sigmas)):
+            npt = shape[0] * shape[1] * shape[2]
+            if jobs and pts + npt > budget:
+                break
+            jobs.append((shape, float(sg), a.seed * 1000 + p, [p], a.tol))
+            pts += npt
+        cpu = cpu_pool_baseline(jobs, False, f"the first {len(jobs)} of the {nprob} problems, solves only "
+                                             "(set-up untimed, as in the batch)")
     print(json.dumps({
         "workload": f"{nprob} problems, dims per axis in {{33,65,129}}, mixed FP32/FP64 to 1e-10 (config 4)",
         "metric": "solves/s", "value": nprob / t_batch, "unit": "solves/s", "ms_per_batch": t_batch * 1e3,
@@ -616,6 +682,7 @@ def run_batch96(a):
         "points_total": int(sum(x * y * z for x, y, z in shapes)), "setup_s_all": setup_s,
         "roofline": {"bound": "hbm", "achieved": alg / t_batch / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / t_batch / 1e9 / peak, "peak_source": kind},
+        "cpu_baseline": cpu,
     }))
 
 
@@ -673,6 +740,23 @@ def run_serve(a):
     out["sequential"] = {"value": nseq / seq, "unit": "solves/s", "s": seq,
                          "sample": f"the first {nseq} of the {len(reqs)} requests"}
     out["speedup_vs_sequential"] = out["value"] / out["sequential"]["value"]
+    if not a.no_cpu_baseline:
+        # A bounded sample of the requests in arrival order (about 4 million
+        # points per host process); a problem's requests go to one process,
+        # which sets it up once and solves each right-hand side.
+        budget, groups, pts = 4e6 * max(1, min(os.cpu_count() or 1, 16)), {}, 0
+        nreq = 0
+        for r in reqs:
+            npt = r.shape[0] * r.shape[1] * r.shape[2]
+            if groups and pts + npt > budget:
+                break
+            m, n, o = r.shape
+            fseed = 1000 + 7919 * r.field + 31 * m + 17 * n + o  # FieldPool's seed of that field
+            groups.setdefault(r.problem, [r.shape, r.sigma, fseed, [], 1e-10])[3].append(r.rhs_seed)
+            pts += npt
+            nreq += 1
+        out["cpu_baseline"] = cpu_pool_baseline([tuple(g) for g in groups.values()], True,
+                                                f"the first {nreq} of the {len(reqs)} requests, set-up and solves")
     print(json.dumps(out))
 
 
