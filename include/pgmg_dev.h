@@ -381,7 +381,10 @@ pgmg_status pgmg_batch_set_graphs(pgmg_batch *b, int on);
  * (default 1, each problem's iterates those of pgmg_dev_solve_relres with
  * check_every = 1), or 0 for the adaptive schedule of pgmg_dev_solve_relres
  * (in mixed precision the FP32 V-cycles between checks form one refinement
- * step), evaluated per problem on the device. */
+ * step), evaluated per problem on the device; PGMG_OPT_CLUSTER_SIZE: CTAs of
+ * each problem's coarse-tail cluster (1, 2, 4, 8 or 16; default 4, so that
+ * many problems' tails run at once), or 0 for the attached handles' size
+ * (which must then agree).  Results do not depend on it. */
 pgmg_status pgmg_batch_set_option(pgmg_batch *b, int key, long long value);
 
 /* ---- host problem generators (no GPU needed) ---------------------------- */

@@ -68,13 +68,16 @@ __device__ __forceinline__ int map_entry(const BMap* __restrict__ M, int b) {
 
 template <class T>
 __global__ void __launch_bounds__(kBlock) kb_gs_colour(const BSlot<T>* __restrict__ S, const BMap* __restrict__ M,
-                                                       const int* __restrict__ active, int lev, int col) {
+                                                       const int* __restrict__ active, int lev, int col, int rev) {
     pdl_enter();
-    int e = map_entry(M, blockIdx.x);
+    // rev: walk the blocks in reverse, so that consecutive colour passes
+    // alternate direction and each starts on data the previous one left in L2.
+    int bi = rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    int e = map_entry(M, bi);
     int s = M->slot[e];
     if (!active[s]) return;
     const BSlot<T>& B = S[s];
-    long p = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
+    long p = (long)(bi - M->start[e]) * blockDim.x + threadIdx.x;
     const LevelGeom& g = B.g[lev];
     if (p >= (long)g.M2 * g.N2 * g.O2) return;
     gs_colour_at<T>(g, B.x[lev], B.r[lev], B.A[lev], col, p);
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(kBlock) kb_restrict(const BSlot<T>* __restrict
     if (!active[s]) return;
     const BSlot<T>& B = S[s];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
-    restrict_at<T>(B.g[lc - 1], B.g[lc], B.res[lc - 1], B.r[lc], B.x[lc], q);
+    restrict_fast_at<T>(B.g[lc - 1], B.g[lc], B.res[lc - 1], B.r[lc], B.x[lc], q);
 }
 
 template <class T>
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(kBlock) kb_interp(const BSlot<T>* __restrict__
     if (!active[s]) return;
     const BSlot<T>& B = S[s];
     long q = (long)(blockIdx.x - M->start[e]) * blockDim.x + threadIdx.x;
-    interp_at<T>(B.g[lc - 1], B.g[lc], B.x[lc - 1], B.x[lc], q);
+    interp_cube_at<T>(B.g[lc - 1], B.g[lc], B.x[lc - 1], B.x[lc], q);  // q: a cube of level lc-1
 }
 
 // FP64 residual of level 0 (or the source alone when x = 0) with the same
@@ -340,7 +343,12 @@ __global__ void __launch_bounds__(kBlock) kb_begin(LevelGeom g, double* x64, int
 struct pgmg_batch {
     int precision = PGMG_MIXED;
     int device = 0;
-    int csize = 0;
+    // CTAs of each problem's coarse-tail cluster.  Batches hold many small
+    // problems, whose tails run side by side: 4-CTA clusters let four times
+    // as many run at once as the single-problem 16 and were fastest on the
+    // 96-problem workload.  PGMG_OPT_CLUSTER_SIZE 0 follows the handles.
+    int csize = 4;
+    bool csize_fixed = true;
     cudaStream_t stream = nullptr;
     std::vector<pgmg_handle*> slots;  // nullptr = free
     // device memory
@@ -480,7 +488,7 @@ pgmg_status build_shape(pgmg_batch* b) {
             gs.push_back({s, nblk(nc)});
             res.push_back({s, 8 * nblk(nc)});
             rst.push_back({s, nblk(h->L[l + 1].g.npts)});
-            itp.push_back({s, nblk(g.npts)});  // interpolation from l+1 into l
+            itp.push_back({s, nblk(nc)});  // interpolation from l+1 into l, one thread per cube of l
         }
         if (gs.empty()) continue;
         b->map_gs[l] = add_map(b, gs);
@@ -545,7 +553,7 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
         if (b->map_gs[l] < 0) continue;
         for (int sw = 0; sw < b->v_down + l; sw++)
             for (int c = 0; c < 8; c++) {
-                BLAUNCH(map_blocks(b, b->map_gs[l]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l]), b->active, l, c);
+                BLAUNCH(map_blocks(b, b->map_gs[l]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l]), b->active, l, c, c & 1);
             }
         BLAUNCH(map_blocks(b, b->map_res[l]), kBlock, kb_residual<T>, S, M(b->map_res[l]), b->active, l);
         BLAUNCH(map_blocks(b, b->map_rst[l + 1]), kBlock, kb_restrict<T>, S, M(b->map_rst[l + 1]), b->active, l + 1);
@@ -555,6 +563,12 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
         cfg.gridDim = dim3((unsigned)(b->members.size() * b->csize), 1, 1);
         cfg.blockDim = dim3(kClusterThreads, 1, 1);
         cfg.stream = b->stream;
+        // No dynamic shared memory: the tails sweep x from L2.  (The
+        // single-problem shared-memory sweeps were slower here: a batched
+        // problem's tail level gets few sweeps per call, and copying the
+        // level in and staging its stencils cost more than the passes saved
+        // -- 96 mixed problems, 4-CTA clusters: 76.9 ms per batch without,
+        // 87.9 ms with.)
         cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = b->csize;
@@ -575,7 +589,7 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
         BLAUNCH(map_blocks(b, b->map_int[l]), kBlock, kb_interp<T>, S, M(b->map_int[l]), b->active, l);
         for (int sw = 0; sw < b->v_up + l - 1; sw++)
             for (int c = 0; c < 8; c++) {
-                BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, c);
+                BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, c, c & 1);
             }
     }
     int nm = (int)b->members.size();
@@ -768,9 +782,11 @@ pgmg_status pgmg_batch_attach(pgmg_batch* b, int slot, pgmg_handle* h) {
     if (h->v_down != b->v_down || h->v_up != b->v_up)
         return bfail(b, PGMG_ERR_UNSUPPORTED, "batched problems use the batch's sweep counts");
     if (h->device != b->device) return bfail(b, PGMG_ERR_ARG, "problem lives on another device");
-    b->csize = h->cluster_size;
-    for (pgmg_handle* o : b->slots)
-        if (o && o->cluster_size != b->csize) return bfail(b, PGMG_ERR_UNSUPPORTED, "cluster sizes differ");
+    if (!b->csize_fixed) {
+        b->csize = h->cluster_size;
+        for (pgmg_handle* o : b->slots)
+            if (o && o->cluster_size != b->csize) return bfail(b, PGMG_ERR_UNSUPPORTED, "cluster sizes differ");
+    }
     b->slots[slot] = h;
     b->dirty = true;
     return PGMG_OK;
@@ -834,6 +850,25 @@ pgmg_status pgmg_batch_set_option(pgmg_batch* b, int key, long long value) {
         case PGMG_OPT_CHECK_EVERY:
             if (value < 0) return bfail(b, PGMG_ERR_ARG, "check period must be >= 0");
             b->check_every = (int)value;
+            break;
+        case PGMG_OPT_CLUSTER_SIZE:
+            // CTAs of each problem's coarse-tail cluster (0: the attached
+            // handles' size).  Smaller clusters let more problems' tails run
+            // at once.
+            if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
+                return bfail(b, PGMG_ERR_ARG, "cluster size must be 0, 1, 2, 4, 8 or 16");
+            b->csize_fixed = value != 0;
+            if (value) {
+                b->csize = (int)value;
+            } else {
+                b->csize = 0;
+                for (pgmg_handle* o : b->slots)
+                    if (o) {
+                        if (b->csize && o->cluster_size != b->csize)
+                            return bfail(b, PGMG_ERR_UNSUPPORTED, "cluster sizes differ");
+                        b->csize = o->cluster_size;
+                    }
+            }
             break;
         default: return bfail(b, PGMG_ERR_ARG, "unknown batch option %d", key);
     }

@@ -543,10 +543,8 @@ __global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T
 // level), so cube C covers fine 2C and 2C+1 (when < the axis size) on each
 // axis -- every fine point exactly once.
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
-                                                        const T* __restrict__ xcv) {
-    pdl_enter();
-    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void interp_cube_at(const LevelGeom& gf, const LevelGeom& gc, T* __restrict__ xf,
+                                               const T* __restrict__ xcv, long p) {
     if (p >= (long)gf.M2 * gf.N2 * gf.O2) return;
     int Cx, Cy, Cz;
     decode_colour(gf, p, Cx, Cy, Cz);
@@ -574,6 +572,13 @@ __global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom 
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
+                                                        const T* __restrict__ xcv) {
+    pdl_enter();
+    interp_cube_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
 // One axis of a coarse point whose transfer is the interior one: both cubes
 // I-1 and I exist, have their upper point and are not snapped, so the fine
 // points 2I-1, 2I, 2I+1 transfer with weights 1/2, 1, 1/2.
@@ -586,10 +591,8 @@ __device__ __forceinline__ bool inner_axis(int I, int ma) {
 // same contributions in the same order, all 27 loads issued first); the
 // others take restrict_at itself.
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
-                                                          T* __restrict__ rc, T* __restrict__ xc) {
-    pdl_enter();
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void restrict_fast_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
+                                                 T* __restrict__ rc, T* __restrict__ xc, long q) {
     if (q >= gc.npts) return;
     int I, J, K;
     decode_nat(gc, q, I, J, K);
@@ -638,6 +641,13 @@ __global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeo
                         }
     rc[gc.ri(I, J, K)] = acc;
     xc[gc.xi(I, J, K)] = T(0);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
+                                                          T* __restrict__ rc, T* __restrict__ xc) {
+    pdl_enter();
+    restrict_fast_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -90,3 +90,25 @@ def test_batch_adaptive_schedule(precision):
         assert c1[1] == cyc[s] and r1[1] == rr[s]
         assert np.array_equal(G.get_x(0), xb[s])
         C.close()
+
+
+def test_batch_cluster_size_changes_no_result():
+    """The coarse-tail cluster size of a batch (default 4 CTAs per problem)
+    changes no iterate: 1, 4 and 16 CTAs, and the handles' own size, give the
+    same cycles and solutions bit for bit."""
+    out = []
+    for cs in (1, 4, 16, 0):
+        probs = [build(s, P.MIXED, 50 + i) for i, s in enumerate(SHAPES[:5])]
+        B = P.Batch(8, P.MIXED)
+        B.set_option(P.OPT_CLUSTER_SIZE, cs)
+        for s, G in enumerate(probs):
+            B.attach(s, G)
+        cyc, rr = B.solve(1e-10, 60)
+        out.append((cyc[:5].copy(), rr[:5].copy(), [G.get_x(0) for G in probs]))
+        B.close()
+        for G in probs:
+            G.close()
+    for cyc, rr, xs in out[1:]:
+        assert np.array_equal(cyc, out[0][0]) and np.array_equal(rr, out[0][1])
+        for a, b in zip(xs, out[0][2]):
+            assert np.array_equal(a, b)
