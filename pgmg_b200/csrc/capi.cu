@@ -507,15 +507,24 @@ pgmg_status check_begin(pgmg_handle* h) {
     return PGMG_OK;
 }
 
-pgmg_status reduce_and_read(pgmg_handle* h, long nb) {
+// The reduction of a check, enqueued; read_norms waits for it.  Work
+// enqueued between the two runs while the host waits.
+pgmg_status reduce_launch(pgmg_handle* h, long nb) {
     if (!h->norm_pin) {
         LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_dev);
         CK(cudaMemcpyAsync(h->norm_host, h->norm_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
         return PGMG_OK;
     }
     LAUNCH(1, 1024, k_reduce_partials, h->partials, nb, h->norm_pin);
     CK(cudaEventRecord(h->ev_post, h->stream));
+    return PGMG_OK;
+}
+
+pgmg_status read_norms(pgmg_handle* h) {
+    if (!h->norm_pin) {
+        CK(cudaStreamSynchronize(h->stream));
+        return PGMG_OK;
+    }
     CK(cudaEventSynchronize(h->ev_pre));
     cudaError_t e = cudaErrorNotReady;
     for (long i = 0; i < kNormPolls && e == cudaErrorNotReady; i++) e = cudaEventQuery(h->ev_post);
@@ -526,6 +535,11 @@ pgmg_status reduce_and_read(pgmg_handle* h, long nb) {
     return PGMG_OK;
 }
 
+pgmg_status reduce_and_read(pgmg_handle* h, long nb) {
+    TRY(reduce_launch(h, nb));
+    return read_norms(h);
+}
+
 // Norms of a level (FP64 data) into h->norm_host; synchronises.
 pgmg_status norms64(pgmg_handle* h, int l, double* res2, double* rhs2) {
     Level& L = h->L[l];
@@ -534,6 +548,19 @@ pgmg_status norms64(pgmg_handle* h, int l, double* res2, double* rhs2) {
     TRY(reduce_and_read(h, nblk((long)L.g.M2 * L.g.N2 * L.g.O2) * 8));
     if (res2) *res2 = h->norm_host[0];
     if (rhs2) *rhs2 = h->norm_host[1];
+    return PGMG_OK;
+}
+
+// x64 += x32 on level 0 (the FP64 update of iterative refinement).
+pgmg_status add_correction(pgmg_handle* h) {
+    Level& L0 = h->L[0];
+    const LevelGeom& g = L0.g;
+    if (((uintptr_t)L0.x64 | (uintptr_t)L0.x32) & 15) {
+        LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+    } else {
+        long n = g.xsize();
+        LAUNCH(nblk((n + 3) / 4), kBlock, k_add_correction_flat, L0.x64, L0.x32, n);
+    }
     return PGMG_OK;
 }
 
@@ -553,10 +580,10 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
         if (res2) *res2 = h->norm_host[0];
         if (rhs2) *rhs2 = h->norm_host[1];
     }
-    LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
+    CK(cudaMemsetAsync(L0.x32, 0, g.xsize() * sizeof(float), h->stream));  // e = 0 (halo too)
     TRY(wrap_level<float>(h, 0));
     TRY(run_vcycle<float>(h, mode, smoother));
-    LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+    TRY(add_correction(h));
     TRY(wrap_level<double>(h, 0));
     return PGMG_OK;
 }
@@ -1478,8 +1505,34 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             LAUNCH(grid, kBlock, k_residual<double, double, true>, g, L0.x64, L0.r64, L0.A64, nullptr,
                                                                                h->partials);
         }
-        if (check) {
+        // Mixed precision: when this check is expected to find the solve not
+        // yet converged, the next refinement step's first FP32 V-cycle (which
+        // changes only the correction e, never x64) is enqueued before the
+        // host waits for the norms, so the GPU does not idle during the round
+        // trip.  If the check converges after all, that work is simply not
+        // used; the result is the same either way.
+        bool spec = false;
+        if (check && mixed) {
+            TRY(reduce_launch(h, nb));
+            if (nc < max_cycles) {
+                if (zero) {
+                    spec = tol < 1.0;  // x = 0: the relative residual is 1 (unless the source is 0)
+                } else {
+                    double q = plan.rho();
+                    spec = q > 0 && q < 0.9 && plan.last_r > 0 &&
+                           plan.last_r * pow(q, nc - plan.last_n) > kSlack * tol;
+                }
+            }
+            if (spec) {
+                CK(cudaMemsetAsync(L0.x32, 0, g.xsize() * sizeof(float), h->stream));
+                TRY(wrap_level<float>(h, 0));
+                TRY(run_vcycle<float>(h, 0, smoother));
+            }
+            TRY(read_norms(h));
+        } else if (check) {
             TRY(reduce_and_read(h, nb));
+        }
+        if (check) {
             res2 = h->norm_host[0];
             rhs2 = h->norm_host[1];
             rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
@@ -1503,10 +1556,12 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             if (plan.every == 0 && inner > cap) inner = cap;
             if (inner > max_cycles - nc) inner = max_cycles - nc;
             if (inner < 1) inner = 1;
-            LAUNCH(nblk(g.npts), kBlock, k_clear_x<float>, g, L0.x32);
-            TRY(wrap_level<float>(h, 0));
-            for (int i = 0; i < inner; i++) TRY(run_vcycle<float>(h, 0, smoother));
-            LAUNCH(nblk(g.npts), kBlock, k_add_correction, g, L0.x64, L0.x32);
+            if (!spec) {
+                CK(cudaMemsetAsync(L0.x32, 0, g.xsize() * sizeof(float), h->stream));  // e = 0 (halo too)
+                TRY(wrap_level<float>(h, 0));
+            }
+            for (int i = spec ? 1 : 0; i < inner; i++) TRY(run_vcycle<float>(h, 0, smoother));
+            TRY(add_correction(h));
             TRY(wrap_level<double>(h, 0));
             nc += inner;
             continue;
