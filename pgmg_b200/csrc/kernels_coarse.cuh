@@ -319,7 +319,7 @@ __device__ __forceinline__ void c_restrict(const LevelGeom gf, const LevelGeom g
     }
 }
 
-// Same values as k_interp.
+// Same values as k_interp_cube (interp_val's formulas, inlined).
 template <class T>
 __device__ __forceinline__ void c_interp(const LevelGeom gf, const LevelGeom gc, T* xf, const T* xcv, int tid,
                                          int nth) {

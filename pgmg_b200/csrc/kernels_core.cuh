@@ -502,46 +502,18 @@ __device__ __forceinline__ T interp_val(int role, bool full, bool xs, bool ys, b
     return val;
 }
 
-// Interpolation with correction add (region.cc:576-593): each fine point
-// belongs to exactly one 2x2x2 cube (C = t>>1, role t&1 per axis) and gets
-// the value interpolate_full (:752-772) or interpolate_partial (:779-810)
-// would give it -- the two differ in how some sums associate; partial is
-// used on the last cube of every row, row of every slice and slice.
-template <class T>
-__device__ __forceinline__ void interp_at(const LevelGeom& gf, const LevelGeom& gc, T* __restrict__ xf,
-                                          const T* __restrict__ xcv, long q) {
-    if (q >= gf.npts) return;
-    int i, j, k;
-    decode_nat(gf, q, i, j, k);
-    int Cx = i >> 1, Cy = j >> 1, Cz = k >> 1, dx = i & 1, dy = j & 1, dz = k & 1;
-    long b = gc.xi(Cx, Cy, Cz);
-    long sy = gc.mx, sz = gc.mx * gc.my;
-    // Corners outside the coarse grid read the zero halo; the formulas never
-    // use them for fine points that exist.
-    T v[8] = {xcv[b], xcv[b + 1], xcv[b + sy], xcv[b + sy + 1],
-              xcv[b + sz], xcv[b + sz + 1], xcv[b + sz + sy], xcv[b + sz + sy + 1]};
-    // Periodic axes: every cube is full, its upper coarse corner at the last
-    // cube being coarse 0's image in the halo.
-    const bool qx = px(gf), qy = py(gf), qz = pz(gf);
-    bool full = (qx || Cx < cube_last(gf.m)) && (qy || Cy < cube_last(gf.n)) && (qz || Cz < cube_last(gf.o));
-    bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
-    T val = interp_val<T>(dx | (dy << 1) | (dz << 2), full, xs, ys, zs, v);
-    long xf_i = gf.xi(i, j, k);
-    xf[xf_i] = xf[xf_i] + val;
-}
-
-template <class T>
-__global__ void __launch_bounds__(kBlock) k_interp(LevelGeom gf, LevelGeom gc, T* __restrict__ xf,
-                                                   const T* __restrict__ xcv) {
-    pdl_enter();
-    interp_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
-}
-
-// The same interpolation with one thread per cube: its 8 coarse corners are
-// loaded once and its (up to) 8 fine points updated, each with interp_at's
-// value.  Cubes are enumerated like colour points (M2 x N2 x O2 of the fine
-// level), so cube C covers fine 2C and 2C+1 (when < the axis size) on each
-// axis -- every fine point exactly once.
+// Interpolation with correction add (region.cc:576-593), one thread per
+// 2x2x2 cube: each fine point belongs to exactly one cube (C = t>>1, role
+// t&1 per axis) and gets the value interpolate_full (:752-772) or
+// interpolate_partial (:779-810) would give it -- the two differ in how some
+// sums associate; partial is used on the last cube of every row, row of
+// every slice and slice.  The cube's 8 coarse corners are loaded once and its
+// (up to) 8 fine points updated.  Cubes are enumerated like colour points
+// (M2 x N2 x O2 of the fine level), so cube C covers fine 2C and 2C+1 (when
+// < the axis size) on each axis -- every fine point exactly once.  Corners
+// outside the coarse grid read the zero halo (on a periodic axis, the upper
+// corner of the last cube is coarse 0's image there); the formulas never use
+// them for fine points that exist.
 template <class T>
 __device__ __forceinline__ void interp_cube_at(const LevelGeom& gf, const LevelGeom& gc, T* __restrict__ xf,
                                                const T* __restrict__ xcv, long p) {
