@@ -156,12 +156,14 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           solution planes the previous one left in L2
  *                           (default); 0 = always bottom up.  No counterpart
  *                           in the reference.
- *   PGMG_OPT_COARSE_SHARED  1 = the cluster coarse cycle sweeps a level with
- *                           its x held in every CTA's shared memory (levels
- *                           whose halo'd x takes at most 200 KiB), updates
- *                           written to all CTAs through distributed shared
- *                           memory (default); 0 = x read from L2.  Same
- *                           results.  No counterpart in the reference.
+ *   PGMG_OPT_COARSE_SHARED  1 = the cluster coarse cycle sweeps a level from
+ *                           shared memory: every CTA holds a copy of the
+ *                           level's halo'd x and the stencils of the points
+ *                           it owns, and sends each new value to the CTAs
+ *                           whose points read it through distributed shared
+ *                           memory (levels whose copy fits in 200 KiB;
+ *                           default); 0 = x read from L2.  Same results.  No
+ *                           counterpart in the reference.
  *   PGMG_OPT_GS_PREFETCH    8-colour levels of at most this many points load
  *                           each colour pass's stencil coefficients before
  *                           waiting for the previous kernel (with PGMG_OPT_PDL,

@@ -380,7 +380,7 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
         long need = 0;
         for (int l = h->coarse_first; l < h->nl; l++) {
             // The colour-major x copy and the staged stencils, for levels where both fit.
-            long b = cm_copy(h->L[l].g, h->cluster_size).bytes((int)sizeof(T));
+            long b = shared_copy(h->L[l].g, h->cluster_size).bytes((int)sizeof(T));
             if (b <= kCoarseXsMax && b > need) need = b;
         }
         cfg.dynamicSmemBytes = (size_t)need;

@@ -147,14 +147,14 @@ __device__ __forceinline__ unsigned dyn_smem_bytes() {
 
 // Shared-memory copy of a level for c_sweeps_shared: the halo'd x array in
 // its global (natural) layout, then the staged stencils.
-struct CmCopy {
+struct ShCopy {
     long nc;      // colour points per colour
     long chunk;   // colour points owned per CTA
     long xelems;  // elements of the x copy (the halo'd array, rounded up to even)
     __host__ __device__ long bytes(int tsize) const { return (xelems + 8 * 28 * chunk) * tsize; }
 };
-__host__ __device__ inline CmCopy cm_copy(const LevelGeom& g, int csize) {
-    CmCopy c;
+__host__ __device__ inline ShCopy shared_copy(const LevelGeom& g, int csize) {
+    ShCopy c;
     c.nc = (long)g.M2 * g.N2 * g.O2;
     c.chunk = (c.nc + csize - 1) / csize;
     c.xelems = (g.xsize() + 1) & ~1L;
@@ -177,8 +177,8 @@ __host__ __device__ inline CmCopy cm_copy(const LevelGeom& g, int csize) {
 template <class T>
 __device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r, const T* A, int sweeps,
                                              int mode, T* sm, int rank, int csize) {
-    const CmCopy cm = cm_copy(g, csize);
-    const int nc = (int)cm.nc, chunk = (int)cm.chunk;
+    const ShCopy cp = shared_copy(g, csize);
+    const int nc = (int)cp.nc, chunk = (int)cp.chunk;
     const int p = rank * chunk + (int)threadIdx.x;
     const bool have = (int)threadIdx.x < chunk && p < nc;
     int i2 = 0, j2 = 0, k2 = 0;
@@ -186,7 +186,7 @@ __device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r
     // Shared-memory indexes fit in 32 bits (the copies are at most kCoarseXsMax bytes).
     const int mxi = (int)g.mx, szi = (int)(g.mx * g.my);
     const int xc0 = (int)g.xi(2 * i2, 2 * j2, 2 * k2);
-    T* as = sm + cm.xelems;
+    T* as = sm + cp.xelems;
     const int xn = (int)g.xsize();
     for (int e = threadIdx.x; e < xn; e += blockDim.x) sm[e] = __ldcg(x + e);
     auto valid = [&](int col) {
@@ -240,7 +240,7 @@ __device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, co
                                          long long budget, int tid, int nth, T* xs, int rank, int csize) {
     int S = slab_count(g, (int)sizeof(T), budget);
     if (S == 1 && (long)g.M2 * g.N2 * g.O2 <= nth) {
-        if (xs && cm_copy(g, csize).bytes((int)sizeof(T)) <= (long)dyn_smem_bytes())
+        if (xs && shared_copy(g, csize).bytes((int)sizeof(T)) <= (long)dyn_smem_bytes())
             c_sweeps_shared<T>(g, x, r, A, sweeps, mode, xs, rank, csize);
         else
             c_sweeps_owned<T>(g, x, r, A, sweeps, mode, tid);
