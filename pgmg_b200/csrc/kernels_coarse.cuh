@@ -12,8 +12,13 @@
 // Data written by one phase and read by another CTA in a later phase (x, r,
 // the residual scratch) is loaded with ld.global.cg (L2, never a stale L1
 // line); read-only stencils and the coarse inverse go through the normal
-// path.  The arithmetic is the same as the grid kernels' (reference-order,
-// no fused multiply-add), so the cluster path gives bit-identical results.
+// path.  When the kernel is launched with dynamic shared memory, the sweeps
+// of every level whose copy fits run from shared memory instead
+// (c_sweeps_shared): each CTA holds the level's x and its own points'
+// stencils, and new values reach the CTAs that read them through distributed
+// shared memory, ordered by the same release/acquire cluster barriers.  The
+// arithmetic is the same as the grid kernels' (reference-order, no fused
+// multiply-add), so the cluster path gives bit-identical results.
 #pragma once
 #include <cooperative_groups.h>
 
