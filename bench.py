@@ -185,23 +185,66 @@ def reference_cycles(R, tol, max_cycles=100):
         n += 1
 
 
+def reference_solve(R, tol, predicted, max_cycles=100):
+    """One solve from the current x the way the reference's own
+    solve_v_cycles works (multigrid.hh:182-219): the predicted number of
+    V-cycles before the first residual check, then one more cycle per check
+    until the relative residual is below tol.  Returns (cycles, relres)."""
+    rhs2 = R.rhs_l2norm()
+    n = 0
+    for _ in range(predicted):
+        R.v_cycle(0)
+        n += 1
+    while True:
+        rr = np.sqrt(R.l2_error_all() / rhs2)
+        if rr < tol or n >= max_cycles or not np.isfinite(rr):
+            return n, rr
+        R.v_cycle(0)
+        n += 1
+
+
+def reference_discovery(R, tol, max_cycles=100):
+    """A solve from x = 0 with a residual check after every V-cycle, to find
+    the cycle count.  Also returns the time the reference's own solve would
+    take with that count predicted: the source norm, the V-cycles and one
+    final residual check, each measured here (the earlier checks only find
+    the count and are not counted)."""
+    t0 = time.perf_counter()
+    rhs2 = R.rhs_l2norm()
+    t_norm = time.perf_counter() - t0
+    t_cycles = 0.0
+    n = 0
+    while True:
+        t0 = time.perf_counter()
+        rr = np.sqrt(R.l2_error_all() / rhs2)
+        t_check = time.perf_counter() - t0
+        if rr < tol or n >= max_cycles or not np.isfinite(rr):
+            return n, rr, t_norm + t_cycles + t_check
+        t0 = time.perf_counter()
+        R.v_cycle(0)
+        t_cycles += time.perf_counter() - t0
+        n += 1
+
+
 def run_reference(a):
     """--impl reference: the reference's own CPU multigrid (compiled from its
     sources into oracle/_ref with a single-rank MPI shim) on the same 257^3
-    problem.  One untimed full solve from x = 0 gives its cycle count; each
-    warm-up step is one V-cycle.  Each timed step is a full solve when K of
-    them fit in about 150 s, else a bounded sample -- two V-cycles with their
-    residual checks, scaled to the full solve's cycle count -- so that the
-    run stays within a few minutes for any --steps."""
+    problem, whose seeded inputs come from the oracle library's generator
+    (the product library is never loaded).  An untimed solve from x = 0 finds
+    the reference's cycle count; each warm-up step is one V-cycle; each timed
+    step is a full solve from x = 0 with that count predicted, as the
+    reference's solve_v_cycles runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.pyoracle import Reference, ref_available
+    from oracle.pyoracle import Reference, benchmark_problem, ref_available
     if not ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpgmg_ref.so not built"}))
         return
     m = a.size
-    coef, S, r = build_problem(m, a.sigma, a.seed)
+    tg = time.perf_counter()
+    coef, S, r = benchmark_problem(m, m, m, a.sigma, a.seed)
+    gen_s = time.perf_counter() - tg
     t0 = time.perf_counter()
     R = Reference(m, m, m, S, coef, r)
     setup_s = time.perf_counter() - t0
@@ -209,36 +252,30 @@ def run_reference(a):
     zero = np.zeros(m * m * m)
     R.set_x(0, zero)
     t0 = time.perf_counter()
-    cycles, rr = reference_cycles(R, a.tol)
-    full_s = time.perf_counter() - t0
+    cycles, rr, _ = reference_discovery(R, a.tol)
+    discovery_s = time.perf_counter() - t0
     for _ in range(a.warmup):
         R.v_cycle(0)
-    full = a.steps * full_s <= 150.0 or cycles < 2
     times = []
     for _ in range(a.steps):
         R.set_x(0, zero)
         t0 = time.perf_counter()
-        if full:
-            reference_cycles(R, a.tol)
-            times.append(time.perf_counter() - t0)
-        else:
-            rhs2 = R.rhs_l2norm()
-            for _ in range(2):
-                R.l2_error_all() / rhs2
-                R.v_cycle(0)
-            times.append((time.perf_counter() - t0) * cycles / 2)
+        c, rr = reference_solve(R, a.tol, cycles)
+        times.append(time.perf_counter() - t0)
     v = float(np.mean(times))
-    sample = (f"{a.steps} full solves of {cycles} V-cycles with residual checks" if full else
-              f"{a.steps} samples of 2 V-cycles with residual checks, each scaled by the {cycles} cycles of a full "
-              f"solve (one untimed full solve: {full_s:.1f} s)")
+    sample = (f"{a.steps} full solves from x = 0, each {cycles} V-cycles (the count an untimed solve with a check "
+              f"after every cycle found, {discovery_s:.1f} s) then a residual check, as the reference's own "
+              f"solve_v_cycles runs a predicted count")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded kappa field and RHS)",
         "config": {"workload": f"{m}^3 Q1 variable-kappa sigma={a.sigma}, solve to {a.tol} rel residual",
-                   "cycles": cycles, "final_relres": rr, "lu_enabled": R.lu_enabled, "setup_s": setup_s},
+                   "cycles": c, "final_relres": rr, "lu_enabled": R.lu_enabled, "setup_s": setup_s,
+                   "input_generation_s": gen_s, "inputs": "oracle library generator (bit for bit the library's)",
+                   "warmup_step": "one V-cycle", "step_s_min_max": [min(times), max(times)]},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": sample + " on one core; the reference has no threading and no MPI here"},
+                         "sample": sample + "; one core: the reference has no threading and no MPI here"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -383,7 +420,7 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         if coef is None:
             coef, S = P.problem_q1(m, m, m, P.problem_kappa(m, m, m, a.sigma, rep.seed(a.seed), 8.0))
-        cpu = cpu_baseline(a, coef, S, r, G)
+        cpu = cpu_baseline(a, coef, S, r)
 
     if rank == 0:
         line = {
@@ -414,37 +451,26 @@ def run_ours(a):
     rep.close()
 
 
-def cpu_baseline(a, coef, S, r, G):
-    """The reference (oracle/_ref) on one host core: its set-up and two
-    V-cycles at the full size, scaled to a solve by the reference's own cycle
-    count (which the GPU's lexicographic mode reproduces bit for bit)."""
+def cpu_baseline(a, coef, S, r):
+    """The reference (oracle/_ref) on one host core: its set-up (untimed) and
+    one full solve from x = 0 with a residual check after every V-cycle.  The
+    value is that solve as the reference's own solve_v_cycles would run it
+    with the count predicted: the source norm, the V-cycles and the final
+    check, all measured in this solve."""
     from oracle.pyoracle import Reference, ref_available
     if not ref_available():
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "oracle/_ref not built"}
-    import pgmg_b200 as P
     m = a.size
     t0 = time.perf_counter()
     R = Reference(m, m, m, S, coef, r)
     setup_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    R.l2_error_all()
-    R.v_cycle(0)
-    R.v_cycle(0)
-    R.l2_error_all()
-    per_cycle = (time.perf_counter() - t0) / 2
-    # The reference's cycle count: the GPU lexicographic mode with the same
-    # coarse solver reproduces the reference's iterates exactly.
+    R.set_x(0, np.zeros(m * m * m))
+    n_ref, rr, solve_s = reference_discovery(R, a.tol)
     lu = R.lu_enabled
     R.close()
-    L = P.Multigrid(m, m, m, coarse=P.COARSE_LU_EXACT if lu else P.COARSE_GS, smoother=P.SMOOTH_LEX)
-    L.setup_matrices(coef, S)
-    L.setup_fields(r)
-    n_ref, rr = L.solve(a.tol, 100, 1)
-    L.close()
-    return {"value": per_cycle * n_ref, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"reference set-up ({setup_s:.1f} s, untimed) + 2 V-cycles with residual checks "
-                      f"({per_cycle:.2f} s/cycle) x {n_ref} cycles to {a.tol} (the reference's count, "
-                      f"lu_enabled={lu})"}
+    return {"value": solve_s, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"one full solve from x = 0: {n_ref} V-cycles to {rr:.2e} (lu_enabled={lu}); timed: the "
+                      f"source norm, the V-cycles and the final residual check (set-up {setup_s:.1f} s untimed)"}
 
 
 # ----------------------------------------------------------------- other configurations
@@ -580,22 +606,21 @@ def run_large513(a):
 
 def _ref_problem_worker(job):
     """One problem of the batch or serving CPU baseline, in a host process of
-    its own: the problem built with the host generators (the same arrays the
-    device generators give), the reference's set-up, then its V-cycles to tol
+    its own: the problem built with the oracle library's generator (the same
+    arrays the library's host and device generators give), the reference's set-up, then its V-cycles to tol
     for each right-hand side.  Returns (set-up s, [solve s per RHS], cycles)."""
     (m, n, o), sigma, field_seed, rhs_seeds, tol = job
-    import pgmg_b200 as P
-    from oracle.pyoracle import Reference
-    kap = P.problem_kappa(m, n, o, sigma, field_seed, 8.0)
-    coef, S = P.problem_q1(m, n, o, kap)
+    from oracle.pyoracle import Reference, input_kappa, input_q1, input_rhs
+    kap = input_kappa(m, n, o, sigma, field_seed, 8.0)
+    coef, S = input_q1(m, n, o, kap)
     del kap
     t0 = time.perf_counter()
-    R = Reference(m, n, o, S, coef, P.problem_rhs(m, n, o, rhs_seeds[0]))
+    R = Reference(m, n, o, S, coef, input_rhs(m, n, o, rhs_seeds[0]))
     setup = time.perf_counter() - t0
     solves, cycles = [], []
     for k, rs in enumerate(rhs_seeds):
         if k:
-            R.set_r(0, P.problem_rhs(m, n, o, rs))
+            R.set_r(0, input_rhs(m, n, o, rs))
         R.set_x(0, np.zeros(m * n * o))
         t0 = time.perf_counter()
         c, _ = reference_cycles(R, tol)

@@ -318,9 +318,11 @@ pgmg_status pgmg_dev_norms(pgmg_handle *h, int level, double *res2, double *rhs2
  * stream has finished.  It allocates nothing: its partial sums live in a
  * fixed 1 MiB array inside this library that every GPU loading it holds until
  * the process exits, so m*n*o is limited to 16,777,216 points (PGMG_ERR_ARG
- * beyond that, and for host pointers).  The first call on a device looks up
- * that array's device address; make that first call before any stream
- * capture.  All calls on a device share the array (each overwrites every
+ * beyond that, and for host pointers).  The first call in each CUDA context
+ * (a device's primary context, or another context the caller has made
+ * current) looks up that array's device address in that context; make that
+ * first call before any stream capture.  All calls on a device share the
+ * array (each overwrites every
  * partial sum it reads, so nothing has to be cleared): calls that overlap on
  * the GPU race and must be serialised by the caller. */
 pgmg_status pgmg_residual_norms_noalloc(int m, int n, int o, const double *coef27, const double *x,

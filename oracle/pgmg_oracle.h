@@ -13,6 +13,8 @@
 #ifndef PGMG_ORACLE_H
 #define PGMG_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -52,6 +54,13 @@ int orc_solve_v_cycles(orc *h,double p_scale,double *res,long *sweeps);
 void orc_setup_test(orc *h,int ca,int xfield,int l);
 void orc_clear_x(orc *h,int l);
 int orc_guide_pred_iters(orc *h);
+/* Seeded benchmark inputs (oracle/inputs.c): the same arrays as the
+ * library's host generators, bit for bit, so that the reference arm of the
+ * benchmark never loads the product library.  Return 0 on success. */
+int orc_input_gauss(int m,int n,int o,uint64_t seed,double width,double *out);
+int orc_input_kappa(int m,int n,int o,double sigma,uint64_t seed,double width,double *kappa);
+int orc_input_q1(int m,int n,int o,const double *kappa,double *c27,int *S6);
+int orc_input_rhs(int m,int n,int o,uint64_t seed,double *r);
 /* Plain dense LU pieces, exposed for the coarse-solver tests. */
 int orc_dgetrf(int n,double *a,int *ipiv);
 void orc_dgetrs(int n,const double *a,const int *ipiv,double *b);

@@ -188,6 +188,65 @@ def oracle_lib():
     return _oracle_lib
 
 
+def _input_lib():
+    lib = oracle_lib()
+    if not getattr(lib, "_inputs_bound", False):
+        u64 = C.c_uint64
+        lib.orc_input_gauss.restype = C.c_int
+        lib.orc_input_gauss.argtypes = [C.c_int] * 3 + [u64, C.c_double, _dp]
+        lib.orc_input_kappa.restype = C.c_int
+        lib.orc_input_kappa.argtypes = [C.c_int] * 3 + [C.c_double, u64, C.c_double, _dp]
+        lib.orc_input_q1.restype = C.c_int
+        lib.orc_input_q1.argtypes = [C.c_int] * 3 + [C.c_void_p, _dp, _ip]
+        lib.orc_input_rhs.restype = C.c_int
+        lib.orc_input_rhs.argtypes = [C.c_int] * 3 + [u64, _dp]
+        lib._inputs_bound = True
+    return lib
+
+
+def input_gauss(m, n, o, seed, width=8.0):
+    """The normalised Gaussian cell field, (m-1)(n-1)(o-1) values."""
+    out = np.empty((m - 1) * (n - 1) * (o - 1))
+    if _input_lib().orc_input_gauss(m, n, o, seed, width, out):
+        raise ValueError("orc_input_gauss")
+    return out
+
+
+def input_kappa(m, n, o, sigma, seed, width=8.0):
+    """kappa = exp(sigma g) per cell."""
+    out = np.empty((m - 1) * (n - 1) * (o - 1))
+    if _input_lib().orc_input_kappa(m, n, o, sigma, seed, width, out):
+        raise ValueError("orc_input_kappa")
+    return out
+
+
+def input_q1(m, n, o, kappa=None):
+    """Q1 stencils (27 slots per point) and boxes (6 ints per point)."""
+    c = np.empty(27 * m * n * o)
+    S = np.empty(6 * m * n * o, np.int32)
+    kp = None if kappa is None else np.ascontiguousarray(kappa, np.float64)
+    if _input_lib().orc_input_q1(m, n, o, _ptr(kp), c, S):
+        raise ValueError("orc_input_q1")
+    return c, S
+
+
+def input_rhs(m, n, o, seed):
+    """Uniform[-1,1] interior source, zero on the boundary."""
+    out = np.empty(m * n * o)
+    if _input_lib().orc_input_rhs(m, n, o, seed, out):
+        raise ValueError("orc_input_rhs")
+    return out
+
+
+def benchmark_problem(m, n, o, sigma, seed, width=8.0):
+    """Stencils, boxes and source of a seeded variable-kappa Q1 problem, from
+    the oracle library only (the same arrays as the product's generators)."""
+    kap = input_kappa(m, n, o, sigma, seed, width)
+    coef, S = input_q1(m, n, o, kap)
+    del kap
+    return coef, S, input_rhs(m, n, o, seed)
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
@@ -202,6 +261,8 @@ def ref_lib():
         lib.ref_get_A27.restype = C.c_int
         lib.ref_get_A27.argtypes = [C.c_void_p, C.c_int, _dp]
         lib.ref_gs_count.restype = C.c_long
+        lib.ref_fmg_cycle.restype = None
+        lib.ref_fmg_cycle.argtypes = [C.c_void_p]
         _ref_lib = lib
     return _ref_lib
 
@@ -252,9 +313,13 @@ class Reference(_Base):
         c27 = np.ascontiguousarray(c27, np.float64).reshape(-1)
         r = None if r is None else np.ascontiguousarray(r, np.float64)
         x = None if x is None else np.ascontiguousarray(x, np.float64)
+        # S6 and c27 are read during construction only; r and x are copied.
         h = lib.ref_create(m, n, o, int(prd[0]), int(prd[1]), int(prd[2]), S6, c27, _ptr(r), _ptr(x))
         super().__init__(lib, h, m, n, o)
-        self._keep = (S6, c27, r, x)
+
+    def fmg_cycle(self):
+        """multigrid::fmg_cycle (multigrid.cc:109-134)."""
+        self.lib.ref_fmg_cycle(self.h)
 
     @staticmethod
     def gs_count() -> int:

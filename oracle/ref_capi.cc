@@ -67,8 +67,7 @@ struct ref_handle {
 	geometry *gm;
 	array_problem pr;
 	multigrid *mg;
-	std::vector<int> S;
-	std::vector<double> c27,r,x;
+	std::vector<double> r,x;
 };
 
 inline region* lev(ref_handle *h,int l) {return h->mg->reg[l];}
@@ -78,13 +77,13 @@ inline region* lev(ref_handle *h,int l) {return h->mg->reg[l];}
 extern "C" {
 
 /* Builds the reference hierarchy for an m x n x o grid and fills level 0
- * from the given arrays (copied).  r and x may be NULL (zero fields). */
+ * from the given arrays.  S and c27 are read during this call only (the
+ * reference copies the entries into its own storage); r and x are copied and
+ * may be NULL (zero fields). */
 void* ref_create(int m,int n,int o,int xp,int yp,int zp,const int *S,
 		 const double *c27,const double *r,const double *x) {
 	ref_handle *h=new ref_handle;
 	long N=(long)m*n*o;
-	h->S.assign(S,S+6*N);
-	h->c27.assign(c27,c27+27*N);
 	h->r.assign(N,0.);h->x.assign(N,0.);
 	if(r) memcpy(&h->r[0],r,N*sizeof(double));
 	if(x) memcpy(&h->x[0],x,N*sizeof(double));
@@ -92,10 +91,11 @@ void* ref_create(int m,int n,int o,int xp,int yp,int zp,const int *S,
 	array_problem &p=h->pr;
 	p.x_prd=xp!=0;p.y_prd=yp!=0;p.z_prd=zp!=0;
 	p.m=m;p.n=n;p.o=o;
-	p.S=&h->S[0];p.c27=&h->c27[0];p.r=&h->r[0];p.x=&h->x[0];
+	p.S=S;p.c27=c27;p.r=&h->r[0];p.x=&h->x[0];
 	h->mg=new multigrid(p,*h->gm,h->com);
 	h->mg->setup_matrices(p);
 	h->mg->setup_fields(p);
+	p.S=NULL;p.c27=NULL;
 	return h;
 }
 

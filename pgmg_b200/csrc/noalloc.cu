@@ -8,6 +8,7 @@
 // arrays, and keeps its only intermediate data -- one pair of partial sums per
 // thread block -- in a fixed array of this file that every GPU loading the
 // library holds until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -19,14 +20,41 @@ namespace {
 constexpr int kNaBlock = 256;
 constexpr long kNaMaxBlocks = 65536;                  // at most 65536 * 256 = 16,777,216 points
 constexpr long kNaMaxPoints = kNaMaxBlocks * kNaBlock;
-constexpr int kNaMaxDevices = 64;
+constexpr int kNaMaxContexts = 64;
 
 // Per-block partial sums (sum res^2, sum r^2), 1 MiB per device.
 static __device__ __align__(256) double g_na_partials[2 * kNaMaxBlocks];
 
-// Device address of g_na_partials, looked up once per device.
-double* g_na_ptr[kNaMaxDevices] = {};
+// Device address of g_na_partials per CUDA context.  The array's address
+// belongs to the context the module was loaded in: a caller that switches
+// to another context (its own cuCtxCreate context, or the primary context
+// re-created after cudaDeviceReset) gets a fresh look-up, never an address
+// of a context that is gone or not current.
+struct NaEntry {
+    CUcontext ctx;
+    double* ptr;
+};
+NaEntry g_na_cache[kNaMaxContexts] = {};
+int g_na_used = 0;
 std::mutex g_na_mu;
+
+// cuCtxGetCurrent through the runtime's driver entry point, so that the
+// library needs no link-time dependency on the driver library.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
 
 __device__ __forceinline__ void na_sum2(double& a, double& b, double* sh) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -110,30 +138,43 @@ bool on_device(const void* p, int dev) {
 extern "C" pgmg_status pgmg_residual_norms_noalloc(int m, int n, int o, const double* coef27, const double* x,
                                                    const double* r, double* out, void* stream) {
     if (m < 1 || n < 1 || o < 1 || !coef27 || !x || !r || !out) return PGMG_ERR_ARG;
+    // Beyond the fixed scratch (2^24 points): each partial product is
+    // bounded before the next multiplication, so no product can overflow.
+    if (m > kNaMaxPoints || (long)m * n > kNaMaxPoints || (long)m * n * o > kNaMaxPoints) return PGMG_ERR_ARG;
     long npts = (long)m * n * o;
-    if (npts > kNaMaxPoints) return PGMG_ERR_ARG;  // beyond the fixed scratch: 2^24 points
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return PGMG_ERR_NO_DEVICE;
     }
-    if (dev < 0 || dev >= kNaMaxDevices) return PGMG_ERR_UNSUPPORTED;
     if (!on_device(coef27, dev) || !on_device(x, dev) || !on_device(r, dev) || !on_device(out, dev))
         return PGMG_ERR_ARG;
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    if (!get_ctx) return PGMG_ERR_UNSUPPORTED;
     double* part = nullptr;
     {
-        // First call on this device: the address of the fixed array, with
-        // this device current.
+        // The address of the fixed array in the current context, looked up
+        // with that context current on its first call there.
         std::lock_guard<std::mutex> lk(g_na_mu);
-        if (!g_na_ptr[dev]) {
+        CUcontext ctx = nullptr;
+        if (get_ctx(&ctx) != CUDA_SUCCESS || !ctx) return PGMG_ERR_CUDA;
+        for (int e = 0; e < g_na_used && !part; e++)
+            if (g_na_cache[e].ctx == ctx) part = g_na_cache[e].ptr;
+        if (!part) {
             double* p = nullptr;
             if (cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_na_partials) != cudaSuccess || !p) {
                 cudaGetLastError();
                 return PGMG_ERR_CUDA;
             }
-            g_na_ptr[dev] = p;
+            // A full table recycles its oldest entry.
+            int e = g_na_used < kNaMaxContexts ? g_na_used++ : 0;
+            if (e == 0 && g_na_used == kNaMaxContexts) {
+                for (int q = 1; q < kNaMaxContexts; q++) g_na_cache[q - 1] = g_na_cache[q];
+                e = kNaMaxContexts - 1;
+            }
+            g_na_cache[e] = {ctx, p};
+            part = p;
         }
-        part = g_na_ptr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     long nb = (npts + kNaBlock - 1) / kNaBlock;

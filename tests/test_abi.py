@@ -115,3 +115,15 @@ def test_dropin_headers_compile_and_link(tmp_path):
                     os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "dropin_driver.cc"), "-o",
                     str(exe), "-L", os.path.join(ROOT, "pgmg_b200"), "-lpgmg_b200"], check=True)
     assert exe.exists()
+
+
+@pytest.mark.parametrize("mno", [(257, 257, 257), (1 << 21, 1 << 21, 1 << 21), (2**31 - 1, 2**31 - 1, 2**31 - 1),
+                                 (2**31 - 1, 1, 1), (1, 1, 2**31 - 1), (4097, 4097, 1)])
+def test_noalloc_rejects_oversize_before_any_launch(mno):
+    """Grids beyond the allocation-free entry point's fixed scratch are
+    rejected by the argument check, before any pointer is looked at or any
+    kernel launched, including sizes whose point count would overflow a
+    64-bit product.  (The pointers passed are not valid memory.)"""
+    m, n, o = mno
+    fake = C.c_void_p(0x1000)
+    assert P.lib().pgmg_residual_norms_noalloc(m, n, o, fake, fake, fake, fake, None) == 7

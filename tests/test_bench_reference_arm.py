@@ -29,6 +29,19 @@ def test_reference_arm_json_line():
     assert 1 <= d["config"]["cycles"] < 100
 
 
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_reference_arm_loads_no_product_library():
+    """The reference arm builds its inputs with the oracle library's generator:
+    the product library is never mapped into its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--size', '17', '--steps', '1', "
+            "'--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_MAPPED', 'libpgmg_b200' in maps, 'REF_MAPPED', 'libpgmg_ref' in maps)")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "PRODUCT_MAPPED False REF_MAPPED True" in out.stdout, out.stdout[-2000:]
+
+
 def test_reference_arm_other_ranks_print_nothing():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2")
     out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--size", "17", "--steps", "1",
