@@ -180,6 +180,10 @@ def oracle_lib():
         lib.orc_set_slab_budget.argtypes = [C.c_void_p, C.c_longlong]
         lib.orc_set_smoother.restype = None
         lib.orc_set_smoother.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_gauss_seidel_tile.restype = None
+        lib.orc_gauss_seidel_tile.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        lib.orc_set_tile.restype = None
+        lib.orc_set_tile.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_long]
         lib.orc_dgetrf.restype = C.c_int
         lib.orc_dgetrf.argtypes = [C.c_int, _dp, _ip]
         lib.orc_dgetrs.restype = None
@@ -295,8 +299,15 @@ class Oracle(_Base):
     def gauss_seidel_mc8(self, mode=0, level=0):
         self.lib.orc_gauss_seidel_mc8(self.h, mode, level)
 
-    def set_smoother(self, mc8: bool):
+    def set_smoother(self, mc8):
+        """0/False lexicographic, 1/True 8-colour, 2 tiled 8-colour."""
         self.lib.orc_set_smoother(self.h, int(mc8))
+
+    def gauss_seidel_tile(self, mode=0, level=0, ty=4, tz=4):
+        self.lib.orc_gauss_seidel_tile(self.h, mode, level, ty, tz)
+
+    def set_tile(self, ty=4, tz=4, min_points=0):
+        self.lib.orc_set_tile(self.h, ty, tz, min_points)
 
     def set_slab_budget(self, nbytes: int):
         self.lib.orc_set_slab_budget(self.h, int(nbytes))

@@ -553,7 +553,7 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
         if (b->map_gs[l] < 0) continue;
         for (int sw = 0; sw < b->v_down + l; sw++)
             for (int c = 0; c < 8; c++) {
-                BLAUNCH(map_blocks(b, b->map_gs[l]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l]), b->active, l, c, c & 1);
+                BLAUNCH(map_blocks(b, b->map_gs[l]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l]), b->active, l, colour_seq(c), c & 1);
             }
         BLAUNCH(map_blocks(b, b->map_res[l]), kBlock, kb_residual<T>, S, M(b->map_res[l]), b->active, l);
         BLAUNCH(map_blocks(b, b->map_rst[l + 1]), kBlock, kb_restrict<T>, S, M(b->map_rst[l + 1]), b->active, l + 1);
@@ -589,7 +589,7 @@ pgmg_status enqueue_step(pgmg_batch* b, double tol, int max_cycles) {
         BLAUNCH(map_blocks(b, b->map_int[l]), kBlock, kb_interp<T>, S, M(b->map_int[l]), b->active, l);
         for (int sw = 0; sw < b->v_up + l - 1; sw++)
             for (int c = 0; c < 8; c++) {
-                BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, c, c & 1);
+                BLAUNCH(map_blocks(b, b->map_gs[l - 1]), kBlock, kb_gs_colour<T>, S, M(b->map_gs[l - 1]), b->active, l - 1, colour_seq(c), c & 1);
             }
     }
     int nm = (int)b->members.size();

@@ -226,7 +226,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         for (int s = 0; s < sweeps; s++)
             for (int pass = 0; pass < (mode ? 2 : 1); pass++)
                 for (int cc = 0; cc < 8; cc++) {
-                    int col = pass ? 7 - cc : cc;
+                    int col = colour_seq(pass ? 7 - cc : cc);
                     int rev = h->gs_alt ? (cc & 1) : 0;
                     if (h->gs_block == 128)
                         LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col, rev);
@@ -246,7 +246,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         for (int s = 0; s < sweeps; s++)
             for (int pass = 0; pass < (mode ? 2 : 1); pass++)
                 for (int cc = 0; cc < 8; cc++) {
-                    int col = pass ? 7 - cc : cc;
+                    int col = colour_seq(pass ? 7 - cc : cc);
                     int rev = h->gs_alt ? (cc & 1) : 0;
                     if (h->gs_block == 128)
                         LAUNCH(nblk(nc, 128), 128, k_gs_colour_pf<T, 128>, g, v.x, v.r, v.A, col, rev);
@@ -264,7 +264,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 int k2lo = slab_lo(g, sl, S), k2hi = slab_lo(g, sl + 1, S);
                 long np = (long)(k2hi - k2lo) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
-                    int col = pass ? 7 - cc : cc;
+                    int col = colour_seq(pass ? 7 - cc : cc);
                     int rev = h->gs_alt ? (cc & 1) : 0;  // alternate the traversal direction
                     if (g.prd)
                         LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi, rev);
@@ -1050,14 +1050,20 @@ pgmg_status pgmg_dev_get_coef(pgmg_handle* h, int level, double* coef27) {
     if (!coef27) return PGMG_ERR_ARG;
     Level& L = h->L[level];
     const LevelGeom& g = L.g;
-    if ((size_t)(27 * g.npts) <= h->stage_elems) {
-        k_cm_to_coef<double><<<nblk(27 * g.npts), kBlock, 0, h->stream>>>(g, L.A64, h->stage);
+    // Chunked by z-planes through the staging buffer.
+    long plane = 27L * g.m * g.n;
+    int kchunk = (int)(h->stage_elems / plane);
+    if (kchunk < 1) return fail(h, PGMG_ERR_INTERNAL, "staging buffer smaller than one plane");
+    for (int k0 = 0; k0 < g.o; k0 += kchunk) {
+        int k1 = k0 + kchunk < g.o ? k0 + kchunk : g.o;
+        size_t cnt = (size_t)plane * (k1 - k0);
+        k_cm_to_coef<double><<<nblk((long)cnt), kBlock, 0, h->stream>>>(g, k0, k1, L.A64, h->stage);
         CKL();
-        CK(cudaMemcpyAsync(coef27, h->stage, sizeof(double) * 27 * g.npts, cudaMemcpyDefault, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        return PGMG_OK;
+        CK(cudaMemcpyAsync(coef27 + (size_t)plane * k0, h->stage, cnt * sizeof(double), cudaMemcpyDefault,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));  // the staging buffer is reused by the next chunk
     }
-    return fail(h, PGMG_ERR_UNSUPPORTED, "level too large for read-back through the staging buffer");
+    return PGMG_OK;
 }
 
 pgmg_status pgmg_dev_get_boxes(pgmg_handle* h, int level, int* S6) {

@@ -98,7 +98,7 @@ __device__ __forceinline__ void c_sweeps_owned(const LevelGeom g, T* x, const T*
     T rv = T(0), ainv = T(1);
     auto colour_at = [&](int st) {
         int cc = st % per;
-        return cc < 8 ? cc : 15 - cc;
+        return colour_seq(cc < 8 ? cc : 15 - cc);
     };
     auto valid = [&](int col) {
         return have && i0 + (col & 1) < g.m && j0 + ((col >> 1) & 1) < g.n && k0 + (col >> 2) < g.o;
@@ -218,7 +218,7 @@ __device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r
     cluster_sync();
     for (int st = 0; st < total; st++) {
         int cc = st % per;
-        int col = cc < 8 ? cc : 15 - cc;
+        int col = colour_seq(cc < 8 ? cc : 15 - cc);
         if (valid(col)) {
             const T* sp = as + col * 28 * chunk + threadIdx.x;
             const int xc = at(col);
@@ -257,7 +257,7 @@ __device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, co
                 int sl = pass ? S - 1 - ss : ss;
                 long p0 = (long)slab_lo(g, sl, S) * g.M2 * g.N2, p1 = (long)slab_lo(g, sl + 1, S) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
-                    c_colour<T>(g, x, r, A, pass ? 7 - cc : cc, p0, p1, tid, nth);
+                    c_colour<T>(g, x, r, A, colour_seq(pass ? 7 - cc : cc), p0, p1, tid, nth);
                     cluster_sync();
                 }
             }

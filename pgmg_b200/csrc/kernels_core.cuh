@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(1024) k_gs_mc8_block(LevelGeom g, T* x, const 
                 int sl = pass ? S - 1 - ss : ss;
                 long p0 = (long)slab_lo(g, sl, S) * g.M2 * g.N2, p1 = (long)slab_lo(g, sl + 1, S) * g.M2 * g.N2;
                 for (int cc = 0; cc < 8; cc++) {
-                    int col = pass ? 7 - cc : cc;
+                    int col = colour_seq(pass ? 7 - cc : cc);
                     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
                         int i2, j2, k2;
                         decode_colour(g, p, i2, j2, k2);
@@ -679,14 +679,16 @@ __global__ void __launch_bounds__(kBlock) k_coef_to_cm(LevelGeom g, int k0, int 
     A[g.ai(i, j, k, s)] = (T)v;
 }
 
-// Colour-major stencils back to natural 27-slot doubles.
+// Colour-major stencils of planes [k0,k1) back to natural 27-slot doubles
+// (dst holds exactly those planes).
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_cm_to_coef(LevelGeom g, const T* __restrict__ A, double* __restrict__ dst) {
+__global__ void __launch_bounds__(kBlock) k_cm_to_coef(LevelGeom g, int k0, int k1, const T* __restrict__ A,
+                                                       double* __restrict__ dst) {
     long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (q >= g.npts * 27) return;
+    if (q >= (long)g.m * g.n * (k1 - k0) * 27) return;
     long pt = q / 27;
     int s = (int)(q % 27);
-    int i = (int)(pt % g.m); long t = pt / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n);
+    int i = (int)(pt % g.m); long t = pt / g.m; int j = (int)(t % g.n); int k = (int)(t / g.n) + k0;
     dst[q] = (double)A[g.ai(i, j, k, s)];
 }
 

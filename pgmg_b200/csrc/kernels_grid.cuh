@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(512, 2) k_sweeps_grid(LevelGeom g, T* x, const
     int per = mode ? 16 : 8, total = sweeps * per;
     for (int st = 0; st < total; st++) {
         int cc = st % per;
-        int col = cc < 8 ? cc : 15 - cc;
+        int col = colour_seq(cc < 8 ? cc : 15 - cc);
         for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < nc; p += stride)
             gs_point_l2<T>(g, x, r, A, col, p, ps, pk);
         if (st + 1 < total && !grid_sync(bar, expect)) return;
