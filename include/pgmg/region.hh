@@ -215,10 +215,7 @@ class region {
     }
     void clear_x_field() { pgmg_dropin::check(pgmg_dev_clear_x(h, level), h, "clear_x"); }
     void allclear_x_field() { clear_x_field(); }
-    void copy_r_to_x() {
-        std::vector<double> v = get(PGMG_FIELD_R);
-        set(PGMG_FIELD_X, &v[0]);
-    }
+    void copy_r_to_x() { pgmg_dropin::check(pgmg_dev_copy_r_to_x(h, level), h, "copy_r_to_x"); }
     void copy_x_to_r() {
         std::vector<double> v = get(PGMG_FIELD_X);
         set(PGMG_FIELD_R, &v[0]);
@@ -241,9 +238,8 @@ class region {
     double l2_error_all() { return norm(0); }
     double rhs_l2norm() { return norm(1); }
     double l0_error() {
-        std::vector<double> v = get(PGMG_FIELD_RES);
         double e = 0;
-        for (size_t q = 0; q < v.size(); q++) e = std::fabs(v[q]) > e ? std::fabs(v[q]) : e;
+        pgmg_dropin::check(pgmg_dev_l0_error(h, level, &e), h, "l0_error");
         return e;
     }
     double l0_error_all() { return l0_error(); }
@@ -266,18 +262,18 @@ class region {
         pgmg_dropin::check(pgmg_dev_get_field(h, level, PGMG_FIELD_RES, ext_r), h, "get_field");
     }
     void Ax(const double* in, double* out) { pgmg_dropin::check(pgmg_dev_apply(h, level, in, out), h, "apply"); }
+    /* One process, no ghost padding: Ax wraps around periodic axes, which
+     * is what unpadded_Ax does (region.cc:1876-1895). */
     void unpadded_Ax(const double* in, double* out) { Ax(in, out); }
     double source_soln_dot() {
-        std::vector<double> a = get(PGMG_FIELD_X), b = get(PGMG_FIELD_R);
         double s = 0;
-        for (size_t q = 0; q < a.size(); q++) s += a[q] * b[q];
+        pgmg_dropin::check(pgmg_dev_source_soln_dot(h, level, &s), h, "source_soln_dot");
         return s;
     }
     void copy_rhs_to_soln() { copy_r_to_x(); }
     double soln_diff(double* ext_x) {
-        std::vector<double> a = get(PGMG_FIELD_X);
         double d = 0;
-        for (size_t q = 0; q < a.size(); q++) d += (ext_x[q] - a[q]) * (ext_x[q] - a[q]);
+        pgmg_dropin::check(pgmg_dev_soln_diff(h, level, ext_x, &d), h, "soln_diff");
         return d;
     }
     void diagnostic_sums() {

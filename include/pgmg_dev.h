@@ -62,7 +62,8 @@ typedef enum {
 
 /* Smoother of a sweep. */
 enum {
-    PGMG_SMOOTH_MC8 = 0, /* 8-colour Gauss-Seidel, colours (i&1)|(j&1)<<1|(k&1)<<2 */
+    PGMG_SMOOTH_MC8 = 0, /* 8-colour Gauss-Seidel, colours (i&1)|(j&1)<<1|(k&1)<<2
+                            swept in the order 0,6,5,3,7,1,2,4 (even i+j+k first) */
     PGMG_SMOOTH_LEX = 1  /* lexicographic order as region.cc:367-446, by wavefronts */
 };
 
@@ -222,6 +223,18 @@ pgmg_status pgmg_dev_autotune(pgmg_handle *h, int reps, double *ms);
  * than the launch has, so its wait runs out (about a second) and the call
  * returns PGMG_ERR_TIMEOUT with the device usable; otherwise PGMG_OK. */
 pgmg_status pgmg_dev_grid_check(pgmg_handle *h, int level, int run_out);
+/* V-cycle profile (no counterpart in the reference): runs one V-cycle of the
+ * handle's options, each stage launched on its own (no graph), with CUDA
+ * events on the handle's stream between the stages, and writes the stage
+ * times in milliseconds: ms[4*l+0] the pre-smoothing sweeps of level l,
+ * ms[4*l+1] the residual and restriction from level l to l+1, ms[4*l+2] the
+ * interpolation from l+1 back to l, ms[4*l+3] the post-smoothing of level l,
+ * for the levels above the coarse part, and ms[4*16] the coarse part (the
+ * one-cluster tail or the bottom solve); nms >= 65 entries, unused ones 0.
+ * fp32 != 0 profiles the FP32 V-cycle of a PGMG_MIXED handle (its
+ * correction is left in the FP32 solution; the FP64 solution is untouched).
+ * *first_coarse: the first level of the coarse part.  Synchronises. */
+pgmg_status pgmg_dev_profile_vcycle(pgmg_handle *h, int fp32, double *ms, int nms, int *first_coarse);
 pgmg_status pgmg_dev_get_option(pgmg_handle *h, int key, long long *value);
 /* Default smoother of pgmg_dev_vcycle and the solves. */
 pgmg_status pgmg_dev_set_smoother(pgmg_handle *h, int smoother);
@@ -271,8 +284,25 @@ pgmg_status pgmg_dev_get_boxes(pgmg_handle *h, int level, int *S6);
 pgmg_status pgmg_dev_set_field(pgmg_handle *h, int level, int field, const double *src);
 pgmg_status pgmg_dev_get_field(pgmg_handle *h, int level, int field, double *dst);
 /* out = A in on a level, natural order, m*n*o doubles each (region::Ax /
- * mul_A / unpadded_Ax, region.cc:1861-1912; multigrid.hh:226-234). */
+ * mul_A / unpadded_Ax, region.cc:1861-1912; multigrid.hh:226-234); on a
+ * periodic axis neighbours wrap around, as in unpadded_Ax. */
 pgmg_status pgmg_dev_apply(pgmg_handle *h, int level, const double *in, double *out);
+/* PCG helpers of the reference's single-process path, computed on the
+ * device (deterministic reductions: the same value on every call):
+ *   pgmg_dev_source_soln_dot  *out = sum x*r     (region::source_soln_dot,
+ *                             region.cc:1921-1931; multigrid.hh:240-242)
+ *   pgmg_dev_soln_diff        *out = sum (ext_x - x)^2, ext_x natural order,
+ *                             host or device (region::soln_diff,
+ *                             region.hh:226-236; multigrid.hh:249-251)
+ *   pgmg_dev_l0_error         *out = max |r - A x| (region::l0_error_all,
+ *                             region.cc:1492-1506), bit for bit the reference's
+ *   pgmg_dev_copy_r_to_x      x = r (region::copy_rhs_to_soln, region.cc:1935-1942)
+ * The sums add the same terms as the reference in another order (1e-12
+ * relative agreement). */
+pgmg_status pgmg_dev_source_soln_dot(pgmg_handle *h, int level, double *out);
+pgmg_status pgmg_dev_soln_diff(pgmg_handle *h, int level, const double *ext_x, double *out);
+pgmg_status pgmg_dev_l0_error(pgmg_handle *h, int level, double *out);
+pgmg_status pgmg_dev_copy_r_to_x(pgmg_handle *h, int level);
 /* x = 0 on a level (region::clear_x_field, region.cc:1679-1682). */
 pgmg_status pgmg_dev_clear_x(pgmg_handle *h, int level);
 /* Analytic test fields (region::setup_test, region.cc:1812-1826). */

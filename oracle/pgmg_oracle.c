@@ -47,10 +47,8 @@ struct orc {
 	int period,iter,use_avg,tol_set;
 	double iter_avg,iter_var,alpha,tol;
 	int v_down,v_up,v_bottom;
-	int smoother;  /* 0 = lexicographic (reference), 1 = 8-colour, 2 = tiled 8-colour */
+	int smoother;  /* 0 = lexicographic (reference), 1 = 8-colour */
 	long long slab_budget;  /* bytes of FP64 x per z-slab of the 8-colour sweep */
-	int tile_ty,tile_tz;    /* tile rows and planes of the tiled sweep */
-	long tile_min;          /* levels of at least this many points use it */
 };
 
 static inline long xi(const olev *L,int i,int j,int k) {
@@ -294,8 +292,6 @@ orc* orc_create(int m,int n,int o,const int *S6,const double *c27,const double *
 	/* multigrid ctor defaults, multigrid.hh:283-285 */
 	h->v_down=2;h->v_bottom=20;h->v_up=2;
 	h->slab_budget=0;
-	h->tile_ty=h->tile_tz=4;
-	h->tile_min=0;
 	/* mg_guide(), multigrid.hh:79-82, set_period :107-111 */
 	h->period=16;h->iter=16;h->iter_avg=16;h->iter_var=1000000;h->alpha=3.0/16;
 	level_alloc(&h->L[0],m,n,o);
@@ -393,38 +389,6 @@ void orc_gauss_seidel_mc8(orc *h,int mode,int l) {
 
 void orc_set_slab_budget(orc *h,long long bytes) {h->slab_budget=bytes;}
 
-/* The tiled 8-colour sweep of this library (not in the reference): the
- * level is cut into tiles of whole x rows, ty rows and tz planes; tile
- * (j0/ty, k0/tz) has tile colour ((j0/ty)&1)|((k0/tz)&1)<<1.  Tiles of one
- * tile colour are never adjacent, so each is swept on its own: for tile
- * colours 0..3, for every tile of that colour, the 8 point colours of the
- * tile in order 0..7 (everything reversed for the backward half of mode !=
- * 0).  Every point is updated once per pass with the latest values of its
- * neighbours in that order, so it is a Gauss-Seidel sweep. */
-void orc_gauss_seidel_tile(orc *h,int mode,int l,int ty,int tz) {
-	olev *L=&h->L[l];
-	int nty=(L->n+ty-1)/ty,ntz=(L->o+tz-1)/tz;
-	h->gs_num++;
-	for(int pass=0;pass<(mode?2:1);pass++)
-	for(int tt=0;tt<4;tt++) {
-		int tc=pass?3-tt:tt;
-		for(int bz=0;bz<ntz;bz++) for(int by=0;by<nty;by++) {
-			if(((by&1)|((bz&1)<<1))!=tc) continue;
-			int j0=by*ty,k0=bz*tz;
-			for(int cc=0;cc<8;cc++) {
-				int c=colour_seq[pass?7-cc:cc];
-				int a=c&1,b=(c>>1)&1,e=(c>>2)&1;
-				for(int k=k0+e;k<k0+tz&&k<L->o;k+=2)
-				for(int j=j0+b;j<j0+ty&&j<L->n;j+=2)
-				for(int i=a;i<L->m;i+=2) gs_point(L,i,j,k);
-			}
-		}
-	}
-}
-
-void orc_set_tile(orc *h,int ty,int tz,long min_points) {
-	h->tile_ty=ty;h->tile_tz=tz;h->tile_min=min_points;
-}
 
 /* region::restriction (region.cc:546-572) with restrict_full/partial
  * (:818-912): clear the coarse r, then for each fine point in cube scan
@@ -504,12 +468,10 @@ void orc_interpolation(orc *h,int l) {
 }
 
 static void gs_any(orc *h,int mode,int l) {
-	if(h->smoother==2&&h->L[l].N>=h->tile_min) orc_gauss_seidel_tile(h,mode,l,h->tile_ty,h->tile_tz);
-	else if(h->smoother) orc_gauss_seidel_mc8(h,mode,l);
-	else orc_gauss_seidel(h,mode,l);
+	if(h->smoother) orc_gauss_seidel_mc8(h,mode,l); else orc_gauss_seidel(h,mode,l);
 }
 
-void orc_set_smoother(orc *h,int mc8) {h->smoother=mc8==2?2:(mc8?1:0);}
+void orc_set_smoother(orc *h,int mc8) {h->smoother=mc8?1:0;}
 
 /* region::solve_exact (region_tr.cc:540-558): LU solve if enabled, else
  * pgmg_gs_exact plain sweeps (of the selected smoother). */

@@ -39,18 +39,11 @@ void orc_get_A27(orc *h,int l,double *out);
 void orc_gauss_seidel(orc *h,int mode,int l);
 void orc_gauss_seidel_mc8(orc *h,int mode,int l);
 /* Smoother of orc_v_cycle and of the coarse fallback sweeps: 0 = the
- * reference's lexicographic Gauss-Seidel (default), 1 = 8-colour, 2 = tiled
- * 8-colour on levels of at least the orc_set_tile size, 8-colour below. */
+ * reference's lexicographic Gauss-Seidel (default), 1 = 8-colour. */
 void orc_set_smoother(orc *h,int mc8);
 /* Slab budget of the 8-colour sweep in bytes of FP64 solution vector
  * (default 0 = one slab, the library's default). */
 void orc_set_slab_budget(orc *h,long long bytes);
-/* Tiled 8-colour sweep: tiles of whole x rows, ty rows and tz planes, four
- * tile colours by (tile row, tile plane) parity, the 8 point colours inside
- * each tile.  orc_set_tile chooses the tile and the smallest level (in
- * points) that smoother 2 sweeps this way (smaller levels: 8-colour). */
-void orc_gauss_seidel_tile(orc *h,int mode,int l,int ty,int tz);
-void orc_set_tile(orc *h,int ty,int tz,long min_points);
 void orc_restriction(orc *h,int l);
 void orc_interpolation(orc *h,int l);
 void orc_solve_exact(orc *h,int l);

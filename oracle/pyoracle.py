@@ -180,10 +180,6 @@ def oracle_lib():
         lib.orc_set_slab_budget.argtypes = [C.c_void_p, C.c_longlong]
         lib.orc_set_smoother.restype = None
         lib.orc_set_smoother.argtypes = [C.c_void_p, C.c_int]
-        lib.orc_gauss_seidel_tile.restype = None
-        lib.orc_gauss_seidel_tile.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
-        lib.orc_set_tile.restype = None
-        lib.orc_set_tile.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_long]
         lib.orc_dgetrf.restype = C.c_int
         lib.orc_dgetrf.argtypes = [C.c_int, _dp, _ip]
         lib.orc_dgetrs.restype = None
@@ -267,6 +263,20 @@ def ref_lib():
         lib.ref_gs_count.restype = C.c_long
         lib.ref_fmg_cycle.restype = None
         lib.ref_fmg_cycle.argtypes = [C.c_void_p]
+        for name in ("ref_compute_residual",):
+            getattr(lib, name).restype = None
+            getattr(lib, name).argtypes = [C.c_void_p, _dp]
+        for name in ("ref_Ax", "ref_unpadded_Ax"):
+            getattr(lib, name).restype = None
+            getattr(lib, name).argtypes = [C.c_void_p, _dp, _dp]
+        lib.ref_source_soln_dot.restype = C.c_double
+        lib.ref_source_soln_dot.argtypes = [C.c_void_p]
+        lib.ref_soln_diff.restype = C.c_double
+        lib.ref_soln_diff.argtypes = [C.c_void_p, _dp]
+        lib.ref_copy_rhs_to_soln.restype = None
+        lib.ref_copy_rhs_to_soln.argtypes = [C.c_void_p]
+        lib.ref_l0_error_all.restype = C.c_double
+        lib.ref_l0_error_all.argtypes = [C.c_void_p, C.c_int]
         _ref_lib = lib
     return _ref_lib
 
@@ -299,15 +309,8 @@ class Oracle(_Base):
     def gauss_seidel_mc8(self, mode=0, level=0):
         self.lib.orc_gauss_seidel_mc8(self.h, mode, level)
 
-    def set_smoother(self, mc8):
-        """0/False lexicographic, 1/True 8-colour, 2 tiled 8-colour."""
+    def set_smoother(self, mc8: bool):
         self.lib.orc_set_smoother(self.h, int(mc8))
-
-    def gauss_seidel_tile(self, mode=0, level=0, ty=4, tz=4):
-        self.lib.orc_gauss_seidel_tile(self.h, mode, level, ty, tz)
-
-    def set_tile(self, ty=4, tz=4, min_points=0):
-        self.lib.orc_set_tile(self.h, ty, tz, min_points)
 
     def set_slab_budget(self, nbytes: int):
         self.lib.orc_set_slab_budget(self.h, int(nbytes))
@@ -331,6 +334,30 @@ class Reference(_Base):
     def fmg_cycle(self):
         """multigrid::fmg_cycle (multigrid.cc:109-134)."""
         self.lib.ref_fmg_cycle(self.h)
+
+    # PCG helpers of level 0 (region.cc:1848-1940, multigrid.hh:222-251).
+    def compute_residual(self):
+        out = np.zeros(self.npts(0))
+        self.lib.ref_compute_residual(self.h, out)
+        return out
+
+    def Ax(self, v, unpadded=False):
+        out = np.zeros(self.npts(0))
+        f = self.lib.ref_unpadded_Ax if unpadded else self.lib.ref_Ax
+        f(self.h, np.ascontiguousarray(v, np.float64), out)
+        return out
+
+    def source_soln_dot(self):
+        return self.lib.ref_source_soln_dot(self.h)
+
+    def soln_diff(self, ext_x):
+        return self.lib.ref_soln_diff(self.h, np.ascontiguousarray(ext_x, np.float64).copy())
+
+    def copy_rhs_to_soln(self):
+        self.lib.ref_copy_rhs_to_soln(self.h)
+
+    def l0_error_all(self, level=0):
+        return self.lib.ref_l0_error_all(self.h, level)
 
     @staticmethod
     def gs_count() -> int:

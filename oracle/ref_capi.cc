@@ -189,6 +189,17 @@ int ref_solve_v_cycles(void *hv,double p_scale,double *res,long *sweeps) {
 	return st;
 }
 
+/* The reference's PCG helpers on level 0 (region.cc:1848-1940,
+ * region.hh:226-236, multigrid.hh:222-251); arrays in natural order (on one
+ * non-periodic process the reference's x layout is natural order). */
+void ref_compute_residual(void *hv,double *out) {static_cast<ref_handle*>(hv)->mg->compute_residual(out);}
+void ref_Ax(void *hv,const double *in,double *out) {static_cast<ref_handle*>(hv)->mg->Ax(in,out);}
+void ref_unpadded_Ax(void *hv,const double *in,double *out) {static_cast<ref_handle*>(hv)->mg->unpadded_Ax(in,out);}
+double ref_source_soln_dot(void *hv) {return static_cast<ref_handle*>(hv)->mg->source_soln_dot();}
+double ref_soln_diff(void *hv,double *ext_x) {return static_cast<ref_handle*>(hv)->mg->soln_diff(ext_x);}
+void ref_copy_rhs_to_soln(void *hv) {static_cast<ref_handle*>(hv)->mg->copy_rhs_to_soln();}
+double ref_l0_error_all(void *hv,int l) {return static_cast<ref_handle*>(hv)->mg->l0_error_all(l);}
+
 int ref_guide_pred_iters(void *hv) {return static_cast<ref_handle*>(hv)->mg->guide.pred_iters();}
 
 long ref_gs_count() {return region::gs_num;}

@@ -99,6 +99,11 @@ SIGNATURES = [
     ("pgmg_dev_coarse_solve", C.c_int, [_VP]),
     ("pgmg_dev_vcycle", C.c_int, [_VP, C.c_int, C.c_int]),
     ("pgmg_dev_fmg_cycle", C.c_int, [_VP, C.c_int]),
+    ("pgmg_dev_profile_vcycle", C.c_int, [_VP, C.c_int, _dp, C.c_int, C.POINTER(C.c_int)]),
+    ("pgmg_dev_source_soln_dot", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
+    ("pgmg_dev_soln_diff", C.c_int, [_VP, C.c_int, _VP, C.POINTER(C.c_double)]),
+    ("pgmg_dev_l0_error", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
+    ("pgmg_dev_copy_r_to_x", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_norms", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pgmg_dev_solve_v_cycles", C.c_int, [_VP, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("pgmg_dev_solve_relres", C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
@@ -460,6 +465,43 @@ class Multigrid:
     def fmg_cycle(self, smoother: int | None = None):
         s = -1 if smoother is None else smoother
         self._ck(lib().pgmg_dev_fmg_cycle(self._h, s), "fmg_cycle")
+
+    def source_soln_dot(self, level: int = 0) -> float:
+        """sum x*r on a level (region::source_soln_dot)."""
+        v = C.c_double(0)
+        self._ck(lib().pgmg_dev_source_soln_dot(self._h, level, C.byref(v)), "source_soln_dot")
+        return v.value
+
+    def soln_diff(self, ext_x, level: int = 0) -> float:
+        """sum (ext_x - x)^2 (region::soln_diff); ext_x natural order."""
+        e = np.ascontiguousarray(ext_x, np.float64)
+        v = C.c_double(0)
+        self._ck(lib().pgmg_dev_soln_diff(self._h, level, e.ctypes.data, C.byref(v)), "soln_diff")
+        return v.value
+
+    def l0_error(self, level: int = 0) -> float:
+        """max |r - A x| (region::l0_error_all)."""
+        v = C.c_double(0)
+        self._ck(lib().pgmg_dev_l0_error(self._h, level, C.byref(v)), "l0_error")
+        return v.value
+
+    def copy_rhs_to_soln(self, level: int = 0):
+        """x = r (region::copy_rhs_to_soln)."""
+        self._ck(lib().pgmg_dev_copy_r_to_x(self._h, level), "copy_r_to_x")
+
+    def profile_vcycle(self, fp32: bool = False) -> dict:
+        """Stage times (ms) of one V-cycle launched stage by stage: per level
+        above the coarse part its pre-sweeps, residual+restriction,
+        interpolation and post-sweeps, and the coarse part."""
+        ms = np.zeros(4 * 16 + 1)
+        fc = C.c_int(0)
+        self._ck(lib().pgmg_dev_profile_vcycle(self._h, int(fp32), ms, len(ms), C.byref(fc)), "profile_vcycle")
+        out = {"levels": [], "coarse_first": fc.value, "coarse_ms": float(ms[64])}
+        for l in range(fc.value):
+            out["levels"].append({"pre_ms": float(ms[4 * l]), "restrict_ms": float(ms[4 * l + 1]),
+                                  "interp_ms": float(ms[4 * l + 2]), "post_ms": float(ms[4 * l + 3])})
+        out["total_ms"] = float(ms.sum())
+        return out
 
     def norms(self, level: int = 0):
         a, b = C.c_double(), C.c_double()

@@ -449,6 +449,43 @@ pgmg_status vcycle_t(pgmg_handle* h, int mode, int smoother) {
     return PGMG_OK;
 }
 
+// vcycle_t with an event recorded after each stage (ev[0] before the first);
+// returns the number of events recorded into ev, and the coarse level.
+template <class T>
+pgmg_status vcycle_profiled(pgmg_handle* h, int smoother, std::vector<cudaEvent_t>& ev, std::vector<int>& tag,
+                            int* lc_out) {
+    int ml = h->nl;
+    bool cl = smoother == PGMG_SMOOTH_MC8 && h->cluster_size > 0 && h->dims.coarse != PGMG_COARSE_LU_EXACT;
+    int lc = cl ? h->coarse_first : ml;
+    int top = lc < ml ? lc : ml - 1;
+    *lc_out = top;
+    auto mark = [&](int t) -> pgmg_status {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ev.push_back(e);
+        tag.push_back(t);
+        CK(cudaEventRecord(e, h->stream));
+        return PGMG_OK;
+    };
+    TRY(mark(-1));
+    for (int i = 0; i < top; i++) {
+        TRY(gs_level<T>(h, i, 0, smoother, h->v_down + i));
+        TRY(mark(4 * i + 0));
+        TRY(restrict_level<T>(h, i + 1));
+        TRY(mark(4 * i + 1));
+    }
+    if (lc < ml) TRY(launch_coarse<T>(h, lc, 0));
+    else TRY(coarse_solve_t<T>(h, smoother));
+    TRY(mark(4 * kMaxLevels));
+    for (int i = top; i > 0; i--) {
+        TRY(interp_level<T>(h, i));
+        TRY(mark(4 * (i - 1) + 2));
+        TRY(gs_level<T>(h, i - 1, 0, smoother, h->v_up + i - 1));
+        TRY(mark(4 * (i - 1) + 3));
+    }
+    return PGMG_OK;
+}
+
 void drop_graphs(pgmg_handle* h) {
     for (int a = 0; a < 2; a++)
         for (int b = 0; b < 2; b++)
@@ -1124,6 +1161,60 @@ pgmg_status pgmg_dev_apply(pgmg_handle* h, int level, const double* in, double* 
     return PGMG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// One PCG helper reduction (k_helper_partials) over a level, read back.
+pgmg_status helper_reduce(pgmg_handle* h, int level, int what, const double* ext, double* out) {
+    Level& L = h->L[level];
+    const LevelGeom& g = L.g;
+    long nb = nblk(g.npts);
+    k_helper_partials<<<(unsigned)nb, kBlock, 0, h->stream>>>(g, L.x64, L.r64, L.A64, ext, what, h->partials);
+    CKL();
+    if (what == 2) k_reduce_max<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+    else k_reduce_partials<<<1, 1024, 0, h->stream>>>(h->partials, nb, h->norm_dev);
+    CKL();
+    double v[2] = {0, 0};
+    CK(cudaMemcpyAsync(v, h->norm_dev, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = v[0];
+    return PGMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pgmg_status pgmg_dev_source_soln_dot(pgmg_handle* h, int level, double* out) {
+    TRY(check_level(h, level));
+    if (!out) return PGMG_ERR_ARG;
+    return helper_reduce(h, level, 0, nullptr, out);
+}
+
+pgmg_status pgmg_dev_soln_diff(pgmg_handle* h, int level, const double* ext_x, double* out) {
+    TRY(check_level(h, level));
+    if (!out || !ext_x) return PGMG_ERR_ARG;
+    const LevelGeom& g = h->L[level].g;
+    CK(cudaMemcpyAsync(h->stage, ext_x, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    return helper_reduce(h, level, 1, h->stage, out);
+}
+
+pgmg_status pgmg_dev_l0_error(pgmg_handle* h, int level, double* out) {
+    TRY(check_level(h, level));
+    if (!out) return PGMG_ERR_ARG;
+    return helper_reduce(h, level, 2, nullptr, out);
+}
+
+pgmg_status pgmg_dev_copy_r_to_x(pgmg_handle* h, int level) {
+    TRY(check_level(h, level));
+    h->x0_zero = false;
+    Level& L = h->L[level];
+    k_r_to_x<double><<<nblk(L.g.npts), kBlock, 0, h->stream>>>(L.g, L.r64, L.x64);
+    CKL();
+    return wrap_level<double>(h, level);
+}
+
 pgmg_status pgmg_dev_clear_x(pgmg_handle* h, int level) {
     TRY(check_level(h, level));
     if (level == 0) h->x0_zero = true;
@@ -1243,6 +1334,32 @@ pgmg_status pgmg_dev_grid_check(pgmg_handle* h, int level, int run_out) {
     if (st == PGMG_OK) st = check_grid(h);
     h->grid_max = keep;
     return st;
+}
+
+pgmg_status pgmg_dev_profile_vcycle(pgmg_handle* h, int fp32, double* ms, int nms, int* first_coarse) {
+    if (!h || !ms || nms < 4 * kMaxLevels + 1) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (fp32 && h->dims.precision != PGMG_MIXED) return fail(h, PGMG_ERR_ARG, "fp32 profile needs a mixed handle");
+    for (int q = 0; q < nms; q++) ms[q] = 0;
+    TRY(upload_plans(h));
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> tag;
+    int lc = 0;
+    h->x0_zero = false;
+    pgmg_status st = fp32 ? vcycle_profiled<float>(h, h->dims.smoother, ev, tag, &lc)
+                          : vcycle_profiled<double>(h, h->dims.smoother, ev, tag, &lc);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (st == PGMG_OK && e == cudaSuccess) {
+        for (size_t q = 1; q < ev.size(); q++) {
+            float t = 0;
+            if (cudaEventElapsedTime(&t, ev[q - 1], ev[q]) == cudaSuccess) ms[tag[q]] += t;
+        }
+    }
+    for (cudaEvent_t x : ev) cudaEventDestroy(x);
+    if (first_coarse) *first_coarse = lc;
+    TRY(st);
+    CK(e);
+    return check_grid(h);
 }
 
 pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {

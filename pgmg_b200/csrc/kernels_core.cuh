@@ -758,9 +758,11 @@ __global__ void __launch_bounds__(kBlock) k_setup_test(LevelGeom g, T* x, T* r, 
     if (xfield) x[g.xi(i, j, k)] = v; else r[g.ri(i, j, k)] = v;
 }
 
-// out = A in (region::mul_A / Ax, region.cc:1861-1912): natural-order input
-// and output of one level, box-order accumulation; neighbours outside the
-// grid carry zero stencil entries and are skipped.
+// out = A in (region::mul_A / Ax / unpadded_Ax, region.cc:1861-1912):
+// natural-order input and output of one level, box-order accumulation.  On a
+// periodic axis a neighbour outside the grid is its periodic image
+// (unpadded_Ax's non_neg_mod, region.cc:1885-1887); on a non-periodic axis
+// it carries a zero stencil entry and is skipped.
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_apply(LevelGeom g, const T* __restrict__ A, const double* __restrict__ in,
                                                   double* __restrict__ out) {
@@ -770,11 +772,90 @@ __global__ void __launch_bounds__(kBlock) k_apply(LevelGeom g, const T* __restri
     decode_nat(g, q, i, j, k);
     double acc = 0.0;
     for (int s = 0; s < 27; s++) {
-        int ii = i + s % 3 - 1, jj = j + (s / 3) % 3 - 1, kk = k + s / 9 - 1;
+        int ii = wrap(i + s % 3 - 1, g.m, px(g)), jj = wrap(j + (s / 3) % 3 - 1, g.n, py(g)),
+            kk = wrap(k + s / 9 - 1, g.o, pz(g));
         if (ii < 0 || jj < 0 || kk < 0 || ii >= g.m || jj >= g.n || kk >= g.o) continue;
         acc = __dadd_rn(acc, __dmul_rn((double)A[g.ai(i, j, k, s)], in[g.pi(ii, jj, kk)]));
     }
     out[q] = acc;
+}
+
+// Per-block partial sums for the PCG helpers, over the points of a level in
+// natural order (grid over natural points):
+//   what 0: sum x*r            (region::source_soln_dot, region.cc:1921-1931)
+//   what 1: sum (ext - x)^2    (region::soln_diff, region.hh:226-236; ext natural)
+//   what 2: max |r - A x|      (region::l0_error_all, region.cc:1492-1506)
+// written to partials[2*block] (the pair layout of k_reduce_partials).
+static __global__ void __launch_bounds__(kBlock) k_helper_partials(LevelGeom g, const double* __restrict__ x,
+                                                                   const double* __restrict__ r,
+                                                                   const double* __restrict__ A,
+                                                                   const double* __restrict__ ext, int what,
+                                                                   double* __restrict__ partials) {
+    __shared__ double sh[64];
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (q < g.npts) {
+        int i, j, k;
+        decode_nat(g, q, i, j, k);
+        long xc = g.xi(i, j, k);
+        if (what == 0) {
+            v = x[xc] * r[g.ri(i, j, k)];
+        } else if (what == 1) {
+            double d = ext[q] - x[xc];
+            v = d * d;
+        } else {
+            long c = g.cidx(i, j, k);
+            int col = g.colour(i, j, k);
+            const double* Ap = A + (long)col * 27 * g.Nc + c;
+            double acc = 0.0;
+            for (int s = 0; s < 27; s++) acc = __dadd_rn(acc, __dmul_rn(Ap[s * g.Nc], x[xc + slot_off(g, s)]));
+            v = fabs(__dsub_rn(r[(long)col * g.Nc + c], acc));
+        }
+    }
+    if (what == 2) {
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+        if (l == 0) sh[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            v = l < nw ? sh[l] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        }
+    } else {
+        double u = 0;
+        block_sum2(v, u, sh);
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = v;
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// Largest of nb partial values (partials[2*q]) into out[0].
+static __global__ void __launch_bounds__(1024) k_reduce_max(const double* __restrict__ partials, long nb,
+                                                            double* __restrict__ out) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    for (long q = threadIdx.x; q < nb; q += blockDim.x) v = fmax(v, partials[2 * q]);
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < nw ? sh[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        if (l == 0) out[0] = v;
+    }
+}
+
+// x = r on a level (region::copy_rhs_to_soln, region.cc:1935-1942).
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_r_to_x(LevelGeom g, const T* __restrict__ r, T* __restrict__ x) {
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= g.npts) return;
+    int i, j, k;
+    decode_nat(g, q, i, j, k);
+    x[g.xi(i, j, k)] = r[g.ri(i, j, k)];
 }
 
 // Elementwise casts used by mixed precision.
