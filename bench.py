@@ -556,9 +556,67 @@ def run_small65(a):
                       "cycles": cyc, "relres": rr, "steps": a.steps, "warmup": a.warmup, "cpu_baseline": ref}))
 
 
+def _ref_sample_worker(job):
+    """The reference's set-up and two V-cycles (each followed by its residual
+    check) of a seeded variable-kappa problem, in a host process of its own,
+    with inputs from the oracle library's generator.  Returns (set-up s, s
+    per V-cycle with its check, relative residual after the two cycles,
+    lu_enabled)."""
+    m, sigma, seed, tol = job
+    from oracle.pyoracle import Reference, benchmark_problem
+    coef, S, r = benchmark_problem(m, m, m, sigma, seed)
+    t0 = time.perf_counter()
+    R = Reference(m, m, m, S, coef, r)
+    setup = time.perf_counter() - t0
+    del coef, S
+    rhs2 = R.rhs_l2norm()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        R.v_cycle(0)
+        rr = float(np.sqrt(R.l2_error_all() / rhs2))
+    per_cycle = (time.perf_counter() - t0) / 2
+    lu = R.lu_enabled
+    R.close()
+    return setup, per_cycle, rr, lu
+
+
+def large_cpu_baseline(a, m, sigma, seed):
+    """The reference on one host core at m^3: its set-up and two V-cycles
+    (a spawn-started host process, so the 60 GB of the reference's arrays are
+    freed with it), scaled to a solve by the reference's cycle count -- the
+    count of this library's lexicographic mode, whose iterates are the
+    reference's bit for bit (with the coarse solver the reference ended up
+    with)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    import torch
+
+    import pgmg_b200 as P
+    from oracle.pyoracle import ref_available
+    if not ref_available():
+        return None
+    with ProcessPoolExecutor(1, mp_context=mp.get_context("spawn")) as pool:
+        setup, per_cycle, rr2, lu = pool.submit(_ref_sample_worker, (m, sigma, seed, a.tol)).result()
+    L = P.Multigrid(m, m, m, coarse=P.COARSE_LU_EXACT if lu else P.COARSE_GS, smoother=P.SMOOTH_LEX)
+    L.assemble_q1(P.problem_gauss(m, m, m, seed, 8.0), from_log=True, sigma=sigma)
+    L.rhs_uniform(seed)
+    n_ref, rr = L.solve(a.tol, 300, 1)
+    L.close()
+    torch.cuda.empty_cache()
+    return {"value": per_cycle * n_ref, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"reference set-up ({setup:.1f} s, untimed) and 2 V-cycles with residual checks "
+                      f"({per_cycle:.2f} s per cycle, relres {rr2:.2e} after 2) x {n_ref} cycles to {a.tol}, the "
+                      f"reference's count (its iterates reproduced by the lexicographic GPU mode, "
+                      f"lu_enabled={lu})"}
+
+
 def run_large513(a):
     """Config 3: 513^3, sigma 2.3: FP64 and mixed solves to 1e-10, and the
-    error of each against an FP64 solve driven to 1e-13."""
+    error of each against the library's FP64 solve driven to 1e-13 (that FP64
+    path agrees with the reference's own solution driven to 1e-13 within 1e-9
+    at 129^3 and sigma 2.3, tests/test_gpu_benchscale.py); the reference on
+    one host core beside it."""
     import torch
 
     import pgmg_b200 as P
@@ -601,6 +659,10 @@ def run_large513(a):
     out["mixed"]["speedup_vs_fp64"] = out["fp64"]["value"] / out["mixed"]["value"]
     dims = level_dims(m, m, m)
     out["fp64"]["vcycle_roofline_ms"] = vcycle_bytes(dims, 8) / measured_peak_hbm()[0] / 1e6
+    out["reference_solution"]["what"] = ("this library's FP64 solve continued to 1e-13 (its FP64 path is pinned "
+                                         "to the reference's own solution at 129^3, sigma 2.3)")
+    if not a.no_cpu_baseline:
+        out["cpu_baseline"] = large_cpu_baseline(a, m, sigma, a.seed)
     print(json.dumps(out))
 
 

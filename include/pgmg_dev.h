@@ -185,7 +185,19 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           are separated by a grid barrier with a bounded wait
  *                           (a wait that runs out makes the solve return
  *                           PGMG_ERR_TIMEOUT); 0 = off (default).  No
- *                           counterpart in the reference. */
+ *                           counterpart in the reference.
+ *   PGMG_OPT_FUSED_RESTRICT 1 or 2 = the restriction of a non-periodic level
+ *                           computes the fine residuals inside the restriction
+ *                           kernel (tiles of the residual in shared memory, no
+ *                           residual array in device memory; 1: tiles of 32 x 8
+ *                           coarse points over 8 planes, default; 2: 32 x 16
+ *                           over 16); 0 = a residual pass, then the
+ *                           restriction.  Same results bit for bit.
+ *   PGMG_OPT_LU_WINDOW      1 = the coarsest level's LU factorisation keeps its
+ *                           active band window in shared memory (default, where
+ *                           it fits in 220 KiB); 0 = one thread block on the
+ *                           dense matrix in device memory.  Same factors bit
+ *                           for bit.  Takes effect at the next set-up. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -202,14 +214,16 @@ enum {
     PGMG_OPT_INNER_DIGITS = 13,
     PGMG_OPT_GS_ALTERNATE = 14,
     PGMG_OPT_GS_PREFETCH = 15,
-    PGMG_OPT_COARSE_SHARED = 16
+    PGMG_OPT_COARSE_SHARED = 16,
+    PGMG_OPT_FUSED_RESTRICT = 17,
+    PGMG_OPT_LU_WINDOW = 18
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
  * PGMG_OPT_GS_ALTERNATE, PGMG_OPT_GS_PREFETCH, PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE,
- * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL --
+ * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT --
  * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,

@@ -37,6 +37,8 @@ OPT_INNER_DIGITS = 13
 OPT_GS_ALTERNATE = 14
 OPT_GS_PREFETCH = 15
 OPT_COARSE_SHARED = 16
+OPT_FUSED_RESTRICT = 17
+OPT_LU_WINDOW = 18
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -283,7 +285,8 @@ class Multigrid:
     # Result-neutral execution options the autotuner chooses among.
     TUNED_OPTIONS = {"gs_block": OPT_GS_BLOCK, "cluster_size": OPT_CLUSTER_SIZE, "cluster_first": OPT_CLUSTER_FIRST,
                      "pdl": OPT_PDL, "grid_max": OPT_GRID_MAX, "gs_vector": OPT_GS_VECTOR,
-                     "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH}
+                     "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH,
+                     "fused_restrict": OPT_FUSED_RESTRICT}
 
     def autotune(self, reps: int = 3, cache: str = None) -> dict:
         """Times V-cycles under the result-neutral execution options and keeps
@@ -303,7 +306,8 @@ class Multigrid:
                 known = json.load(f)
             if key in known:
                 for name, opt in self.TUNED_OPTIONS.items():
-                    self.set_option(opt, int(known[key][name]))
+                    if name in known[key]:
+                        self.set_option(opt, int(known[key][name]))
                 return dict(known[key], cached=True)
         ms = C.c_double()
         self._ck(lib().pgmg_dev_autotune(self._h, int(reps), C.byref(ms)), "autotune")

@@ -291,11 +291,29 @@ pgmg_status residual_level(pgmg_handle* h, int l, T* out, double* partials) {
     return PGMG_OK;
 }
 
+template <class T, class Tile>
+pgmg_status fused_restrict(pgmg_handle* h, Level& F, Level& Cl, View<T>& vf, View<T>& vc) {
+    const LevelGeom& gc = Cl.g;
+    dim3 grid((unsigned)((gc.m + Tile::tx - 1) / Tile::tx), (unsigned)((gc.n + Tile::ty - 1) / Tile::ty),
+              (unsigned)((gc.o + Tile::kc - 1) / Tile::kc));
+    const size_t sm = Tile::template smem<T>();
+    if (sm > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_resrestrict<T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    h->launches++;
+    CK(launch_k_smem(h->stream, h->pdl, grid, dim3(Tile::threads), sm, k_resrestrict<T, Tile>, F.g, gc,
+                     (const T*)vf.x, (const T*)vf.r, (const T*)vf.A, vc.r, vc.x));
+    return PGMG_OK;
+}
+
 template <class T>
 pgmg_status restrict_level(pgmg_handle* h, int l) {
     Level& F = h->L[l - 1];
     Level& Cl = h->L[l];
     View<T> vf = view<T>(F), vc = view<T>(Cl);
+    if (!F.g.prd && h->fused_restrict) {
+        if (h->fused_restrict == 2) return fused_restrict<T, RrLarge>(h, F, Cl, vf, vc);
+        return fused_restrict<T, RrSmall>(h, F, Cl, vf, vc);
+    }
     TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
     if (F.g.prd)
         LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T, true>, F.g, Cl.g, vf.res, vc.r, vc.x);
@@ -640,7 +658,14 @@ pgmg_status lu_setup(pgmg_handle* h) {
         // axis couples the first and last planes: no band).
         int kb = L.g.prd ? (int)n - 1 : 1 + L.g.m + L.g.m * L.g.n;
         if (kb > (int)n - 1) kb = (int)n - 1;
-        k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
+        size_t wsm = lu_window_smem((int)n, kb, kb);
+        if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax) {
+            // The active band window in shared memory (same factors).
+            CK(cudaFuncSetAttribute(k_lu_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+            k_lu_window<<<1, 1024, wsm, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
+        } else {
+            k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
+        }
         CKL();
     }
     int info = 0;
@@ -722,15 +747,10 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
     h->nl = plan_levels(*dims, g);
     for (int l = 0; l < h->nl; l++) h->L[l].g = g[l];
     h->prd = g[0].prd;
-    // Periodic axes: every level that is smoothed and restricted (all but
-    // the bottom) must be even along them -- the 8-colour order needs the
-    // wrap-around neighbours to differ in parity, and the transfers here
-    // cover even periodic axes (coarse size m/2).
-    for (int l = 0; l + 1 < h->nl; l++)
-        if ((px(g[l]) && (g[l].m & 1)) || (py(g[l]) && (g[l].n & 1)) || (pz(g[l]) && (g[l].o & 1))) {
-            delete h;
-            return PGMG_ERR_UNSUPPORTED;
-        }
+    // Periodic axes of odd size (on any level) are supported: their
+    // transfers follow igrid_map's odd periodic branch, and a level with one
+    // is swept lexicographically (no 8-colouring separates the neighbours
+    // across its seam, which have equal parity).
     carve(h);  // count
     size_t bytes = h->arena.used;
     if (mem) {
@@ -878,6 +898,13 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_COARSE_SHARED:
             h->coarse_shared = value != 0;
             break;
+        case PGMG_OPT_FUSED_RESTRICT:
+            if (value < 0 || value > 2) return fail(h, PGMG_ERR_ARG, "fused restriction must be 0, 1 or 2");
+            h->fused_restrict = (int)value;
+            break;
+        case PGMG_OPT_LU_WINDOW:
+            h->lu_window = value != 0;
+            break;
         case PGMG_OPT_GS_PREFETCH:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
             h->gs_prefetch = value;
@@ -929,6 +956,8 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_GS_ALTERNATE: *value = h->gs_alt; return PGMG_OK;
         case PGMG_OPT_GS_PREFETCH: *value = h->gs_prefetch; return PGMG_OK;
         case PGMG_OPT_COARSE_SHARED: *value = h->coarse_shared; return PGMG_OK;
+        case PGMG_OPT_FUSED_RESTRICT: *value = h->fused_restrict; return PGMG_OK;
+        case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1056,11 +1085,16 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
         Level& Cl = h->L[l];
         k_rat_bounds<<<nblk(Cl.g.npts), kBlock, 0, h->stream>>>(F.g, Cl.g, F.S, Cl.S);
         CKL();
-        if (Cl.g.npts <= kRatSmallMax)
+        if (Cl.g.npts <= kRatSmallMax) {
             k_rat_fill_small<<<nblk(Cl.g.npts * 32, kRatSmallBlock), kRatSmallBlock, 0, h->stream>>>(F.g, Cl.g, F.A64,
                                                                                                    F.S, Cl.A64);
-        else
+        } else if (!F.g.prd) {
+            CK(cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem));
+            dim3 grid((unsigned)((Cl.g.m + kRtX - 1) / kRtX), (unsigned)Cl.g.n, (unsigned)((Cl.g.o + kRtKC - 1) / kRtKC));
+            k_rat_tile<<<grid, kRtThreads, kRtSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+        } else {
             k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, 0, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+        }
         CKL();
     }
     if (h->dims.precision == PGMG_MIXED)
@@ -1285,6 +1319,7 @@ struct TuneVal {
     long long grid_max;
     int gs_vec, gs_alt;
     long long gs_prefetch;
+    int fused_restrict;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1299,6 +1334,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->gs_vec = v.gs_vec != 0;
     h->gs_alt = v.gs_alt != 0;
     h->gs_prefetch = v.gs_prefetch;
+    h->fused_restrict = v.fused_restrict;
     drop_graphs(h);
 }
 
@@ -1387,8 +1423,9 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    TuneVal best{h->gs_block, h->coarse_first,  h->cluster_size,   h->pdl ? 1 : 0,         h->grid_max,
-                 h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch, 0};
+    TuneVal best{h->gs_block,         h->coarse_first,   h->cluster_size, h->pdl ? 1 : 0,
+                 h->grid_max,         h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch,
+                 h->fused_restrict, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1460,6 +1497,15 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
             if (gm == g0) continue;
             TuneVal c = best;
             c.grid_max = gm;
+            if ((st = trial(c)) != PGMG_OK) break;
+        }
+    }
+    if (st == PGMG_OK && !h->prd) {
+        int f0 = best.fused_restrict;
+        for (int f : {0, 1, 2}) {
+            if (f == f0) continue;
+            TuneVal c = best;
+            c.fused_restrict = f;
             if ((st = trial(c)) != PGMG_OK) break;
         }
     }

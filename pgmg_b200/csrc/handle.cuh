@@ -71,6 +71,23 @@ cudaError_t launch_k(cudaStream_t stream, bool pdl, dim3 grid, dim3 block, void 
     return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 
+// launch_k with dynamic shared memory.
+template <class... KArgs, class... Args>
+cudaError_t launch_k_smem(cudaStream_t stream, bool pdl, dim3 grid, dim3 block, size_t smem, void (*k)(KArgs...),
+                          Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 }  // namespace pgmg
 
 struct pgmg_handle {
@@ -123,6 +140,13 @@ struct pgmg_handle {
     // Coarse-cycle sweeps keep the level's x in each CTA's shared memory
     // (levels whose halo'd x fits in kCoarseXsMax bytes).
     bool coarse_shared = true;
+    // Non-periodic restrictions compute their residuals inside the kernel
+    // (k_resrestrict; 1: 32 x 8 coarse tiles over 8 planes, 2: 32 x 16 over
+    // 16) instead of a residual pass plus k_restrict_fast (0).
+    int fused_restrict = 1;
+    // The coarse LU factorises in a shared-memory band window (k_lu_window)
+    // where it fits, instead of the one-block kernel on device memory.
+    bool lu_window = true;
     int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident

@@ -410,23 +410,19 @@ static __global__ void __launch_bounds__(1024) k_reduce_partials(const double* _
 // reference's restrict_partial tests the x snap flag for the y axis of the
 // (ti,tj+1,tk+1) point (region.cc:888-895); that is kept, see ysnap below.
 // Also clears the coarse x (multigrid.cc:219).
-template <class T, bool PRD = false>
-__device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
-                                            T* __restrict__ rc, T* __restrict__ xc, long q) {
-    if (q >= gc.npts) return;
-    int I, J, K;
-    decode_nat(gc, q, I, J, K);
+template <class T, bool PRD, class Get>
+__device__ __forceinline__ T restrict_sum(const LevelGeom& gf, int I, int J, int K, Get res) {
     // PRD: the instantiation for levels with periodic axes.
     const bool qx = PRD && px(gf), qy = PRD && py(gf), qz = PRD && pz(gf);
     int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     T acc = T(0);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < cube_first(qz) || cz > lz) continue;
+        if (cz < cube_first(gf.o, qz) || cz > lz) continue;
         bool zsn = snapped(cz, gf.o, qz);
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < cube_first(qy) || cy > ly) continue;
+            if (cy < cube_first(gf.n, qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < cube_first(qx) || cx > lx) continue;
+                if (cx < cube_first(gf.m, qx) || cx > lx) continue;
                 bool xsn = snapped(cx, gf.m, qx);
                 for (int dz = 0; dz < 2; dz++) {
                     if (dz && !has_upper(cz, gf.o, qz)) continue;
@@ -441,7 +437,7 @@ __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom
                             if (w == 0.0) continue;
                             int fi = wrap(2 * cx + dx, gf.m, qx), fj = wrap(2 * cy + dy, gf.n, qy),
                                 fk = wrap(2 * cz + dz, gf.o, qz);
-                            T rd = (T)(0.125 * w) * res[gf.ri(fi, fj, fk)];
+                            T rd = (T)(0.125 * w) * res(fi, fj, fk);
                             acc = add_rn<T>(acc, rd);
                         }
                     }
@@ -449,7 +445,16 @@ __device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom
             }
         }
     }
-    rc[gc.ri(I, J, K)] = acc;
+    return acc;
+}
+
+template <class T, bool PRD = false>
+__device__ __forceinline__ void restrict_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
+                                            T* __restrict__ rc, T* __restrict__ xc, long q) {
+    if (q >= gc.npts) return;
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
+    rc[gc.ri(I, J, K)] = restrict_sum<T, PRD>(gf, I, J, K, [&](int i, int j, int k) { return res[gf.ri(i, j, k)]; });
     xc[gc.xi(I, J, K)] = T(0);
 }
 
@@ -525,7 +530,8 @@ __device__ __forceinline__ void interp_cube_at(const LevelGeom& gf, const LevelG
     T v[8] = {xcv[b], xcv[b + 1], xcv[b + sy], xcv[b + sy + 1],
               xcv[b + sz], xcv[b + sz + 1], xcv[b + sz + sy], xcv[b + sz + sy + 1]};
     const bool qx = px(gf), qy = py(gf), qz = pz(gf);
-    bool full = (qx || Cx < cube_last(gf.m)) && (qy || Cy < cube_last(gf.n)) && (qz || Cz < cube_last(gf.o));
+    bool full = (even_prd(gf.m, qx) || Cx < cube_last(gf.m)) && (even_prd(gf.n, qy) || Cy < cube_last(gf.n)) &&
+                (even_prd(gf.o, qz) || Cz < cube_last(gf.o));
     bool xs = snapped(Cx, gf.m, qx), ys = snapped(Cy, gf.n, qy), zs = snapped(Cz, gf.o, qz);
     int i0 = 2 * Cx, j0 = 2 * Cy, k0 = 2 * Cz;
     long f0 = gf.xi(i0, j0, k0);
@@ -559,38 +565,22 @@ __device__ __forceinline__ bool inner_axis(int I, int ma) {
 }
 
 // Restriction of a non-periodic level.  Coarse points interior on all three
-// axes run restrict_at's loops with the weights known at compile time (the
+// axes run restrict_sum's loops with the weights known at compile time (the
 // same contributions in the same order, all 27 loads issued first); the
-// others take restrict_at itself.
-template <class T>
-__device__ __forceinline__ void restrict_fast_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
-                                                 T* __restrict__ rc, T* __restrict__ xc, long q) {
-    if (q >= gc.npts) return;
-    int I, J, K;
-    decode_nat(gc, q, I, J, K);
-    if (!(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o))) {
-        restrict_at<T, false>(gf, gc, res, rc, xc, q);
-        return;
-    }
+// others take restrict_sum itself.
+template <class T, class Get>
+__device__ __forceinline__ T restrict_fast_sum(const LevelGeom& gf, int I, int J, int K, Get res) {
+    if (!(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o)))
+        return restrict_sum<T, false>(gf, I, J, K, res);
     // Per axis: cube a (0: I-1, 1: I), role d -> fine offset 2a+d-2 from 2I,
     // weight 0 (not visited), 1/2, 1, 1/2.
     T rv[27];
 #pragma unroll
-    for (int az = 0; az < 2; az++)
+    for (int oz = -1; oz <= 1; oz++)
 #pragma unroll
-        for (int ay = 0; ay < 2; ay++)
+        for (int oy = -1; oy <= 1; oy++)
 #pragma unroll
-            for (int ax = 0; ax < 2; ax++)
-#pragma unroll
-                for (int dz = 0; dz < 2; dz++)
-#pragma unroll
-                    for (int dy = 0; dy < 2; dy++)
-#pragma unroll
-                        for (int dx = 0; dx < 2; dx++) {
-                            int oz = 2 * az + dz - 2, oy = 2 * ay + dy - 2, ox = 2 * ax + dx - 2;
-                            if (ox < -1 || oy < -1 || oz < -1) continue;
-                            rv[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)] = res[gf.ri(2 * I + ox, 2 * J + oy, 2 * K + oz)];
-                        }
+            for (int ox = -1; ox <= 1; ox++) rv[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)] = res(2 * I + ox, 2 * J + oy, 2 * K + oz);
     T acc = T(0);
 #pragma unroll
     for (int az = 0; az < 2; az++)
@@ -611,7 +601,16 @@ __device__ __forceinline__ void restrict_fast_at(const LevelGeom& gf, const Leve
                             T rd = (T)(0.125 * w) * rv[(oz + 1) * 9 + (oy + 1) * 3 + (ox + 1)];
                             acc = add_rn<T>(acc, rd);
                         }
-    rc[gc.ri(I, J, K)] = acc;
+    return acc;
+}
+
+template <class T>
+__device__ __forceinline__ void restrict_fast_at(const LevelGeom& gf, const LevelGeom& gc, const T* __restrict__ res,
+                                                 T* __restrict__ rc, T* __restrict__ xc, long q) {
+    if (q >= gc.npts) return;
+    int I, J, K;
+    decode_nat(gc, q, I, J, K);
+    rc[gc.ri(I, J, K)] = restrict_fast_sum<T>(gf, I, J, K, [&](int i, int j, int k) { return res[gf.ri(i, j, k)]; });
     xc[gc.xi(I, J, K)] = T(0);
 }
 
@@ -620,6 +619,95 @@ __global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeo
                                                           T* __restrict__ rc, T* __restrict__ xc) {
     pdl_enter();
     restrict_fast_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// Residual fused with the restriction of a non-periodic level
+// (region::restriction, region.cc:546-572: the residual r - A x of every fine
+// point, region.cc:1833-1842, gathered into the coarse r with the weights of
+// restrict_full/partial, :818-912; the coarse x cleared, multigrid.cc:219),
+// without a residual array in global memory.  A CTA owns a tile of TX x TY
+// coarse points and walks up KC coarse planes.  For coarse plane K it
+// computes the residuals of fine planes 2K and 2K+1 over the tile's fine
+// footprint -- fine x in [2*I0-1, 2*(I0+TX)-1], y likewise -- into a ring
+// of three fine planes in shared memory (plane 2K-1 is kept from the step
+// before), two residuals per thread at a time, then every thread gathers its
+// coarse point's contributions from the ring in the reference's order.  Each
+// residual and each sum is the one k_residual and k_restrict_fast compute,
+// so the coarse source is the same bit for bit.  The footprint's one-point
+// rim is recomputed by the neighbouring tiles, which run at the same time, so
+// its stencils are mostly re-read from L2.  The dynamic shared memory is
+// 3 * (2TY+1) * (2TX+1) values of T.
+template <int TX, int TY, int KC>
+struct RrTile {
+    static constexpr int tx = TX, ty = TY, kc = KC, threads = TX * TY;
+    static constexpr int fx = 2 * TX + 1, fy = 2 * TY + 1;
+    static constexpr int plane = fx * fy;
+    template <class T> static constexpr size_t smem() { return 3 * (size_t)plane * sizeof(T); }
+};
+using RrSmall = RrTile<32, 8, 8>;
+using RrLarge = RrTile<32, 16, 16>;
+
+template <class T, class Tile>
+__global__ void __launch_bounds__(Tile::threads) k_resrestrict(LevelGeom gf, LevelGeom gc, const T* __restrict__ x,
+                                                               const T* __restrict__ r, const T* __restrict__ A,
+                                                               T* __restrict__ rc, T* __restrict__ xc) {
+    extern __shared__ __align__(16) unsigned char rr_raw[];
+    T* ring = reinterpret_cast<T*>(rr_raw);
+    constexpr int FX = Tile::fx, NP = Tile::plane;
+    pdl_enter();
+    const int I0 = blockIdx.x * Tile::tx, J0 = blockIdx.y * Tile::ty, K0 = blockIdx.z * Tile::kc;
+    const int K1 = K0 + Tile::kc < gc.o ? K0 + Tile::kc : gc.o;
+    const int fi0 = 2 * I0 - 1, fj0 = 2 * J0 - 1;
+    const uint64_t ps = policy_evict_first(), pk = policy_evict_last();
+    // Residual of footprint entry w of fine plane fk (false: outside the level).
+    auto point = [&](int w, int fk, long& xcn, const T*& Ap, const T*& rp) -> bool {
+        int fi = fi0 + w % FX, fj = fj0 + w / FX;
+        if (fi < 0 || fi >= gf.m || fj < 0 || fj >= gf.n) return false;
+        int col = gf.colour(fi, fj, fk);
+        long c = gf.cidx(fi, fj, fk);
+        xcn = gf.xi(fi, fj, fk);
+        Ap = A + (long)col * 27 * gf.Nc + c;
+        rp = r + (long)col * gf.Nc + c;
+        return true;
+    };
+    auto fine_plane = [&](int fk) {
+        if (fk < 0 || fk >= gf.o) return;
+        T* dst = ring + (fk % 3) * NP;
+        for (int w0 = threadIdx.x; w0 < NP; w0 += 2 * Tile::threads) {
+            const int w1 = w0 + Tile::threads;
+            long x0 = 0, x1 = 0;
+            const T *A0 = A, *A1 = A, *r0 = r, *r1 = r;
+            const bool v0 = point(w0, fk, x0, A0, r0);
+            const bool v1 = w1 < NP && point(w1, fk, x1, A1, r1);
+            if (!v0) x0 = x1, A0 = A1, r0 = r1;
+            if (!v1) x1 = x0, A1 = A0, r1 = r0;
+            if (!v0 && !v1) continue;
+            T a0 = T(0), a1 = T(0);
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                const long o = slot_off(gf, q);
+                a0 = madd<true, T>(a0, ld_stream(A0 + q * gf.Nc, ps), ld_keep(x + x0 + o, pk));
+                a1 = madd<true, T>(a1, ld_stream(A1 + q * gf.Nc, ps), ld_keep(x + x1 + o, pk));
+            }
+            if (v0) dst[w0] = sub_rn<T>(ld_stream(r0, ps), a0);
+            if (v1) dst[w1] = sub_rn<T>(ld_stream(r1, ps), a1);
+        }
+    };
+    const int I = I0 + (int)threadIdx.x % Tile::tx, J = J0 + (int)threadIdx.x / Tile::tx;
+    fine_plane(2 * K0 - 1);
+    for (int K = K0; K < K1; K++) {
+        fine_plane(2 * K);
+        fine_plane(2 * K + 1);
+        __syncthreads();
+        if (I < gc.m && J < gc.n) {
+            T v = restrict_fast_sum<T>(gf, I, J, K, [&](int i, int j, int k) {
+                return ring[(k % 3) * NP + (j - fj0) * FX + (i - fi0)];
+            });
+            rc[gc.ri(I, J, K)] = v;
+            xc[gc.xi(I, J, K)] = T(0);
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------

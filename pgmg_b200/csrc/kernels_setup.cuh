@@ -21,7 +21,7 @@ __device__ inline AxisList axis_list(int I, int ma, bool p) {
     L.n = 0;
     int last = cube_last(ma, p);
     for (int C = I - 1; C <= I; C++) {
-        if (C < cube_first(p) || C > last) continue;
+        if (C < cube_first(ma, p) || C > last) continue;
         bool sn = snapped(C, ma, p);
         for (int d = 0; d < 2; d++) {
             if (d && !has_upper(C, ma, p)) continue;
@@ -92,11 +92,11 @@ static __global__ void __launch_bounds__(kRatBlock, 4) k_rat_fill(LevelGeom gf, 
     const bool qx = px(gf), qy = py(gf), qz = pz(gf);
     int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < cube_first(qz) || cz > lz) continue;
+        if (cz < cube_first(gf.o, qz) || cz > lz) continue;
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < cube_first(qy) || cy > ly) continue;
+            if (cy < cube_first(gf.n, qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < cube_first(qx) || cx > lx) continue;
+                if (cx < cube_first(gf.m, qx) || cx > lx) continue;
                 for (int dz = 0; dz < 2; dz++) {
                     if (dz && !has_upper(cz, gf.o, qz)) continue;
                     bool zsn = snapped(cz, gf.o, qz);
@@ -187,11 +187,11 @@ static __global__ void __launch_bounds__(kRatSmallBlock, 4) k_rat_fill_small(Lev
     const bool qx = px(gf), qy = py(gf), qz = pz(gf);
     int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     for (int cz = K - 1; cz <= K; cz++) {
-        if (cz < cube_first(qz) || cz > lz) continue;
+        if (cz < cube_first(gf.o, qz) || cz > lz) continue;
         for (int cy = J - 1; cy <= J; cy++) {
-            if (cy < cube_first(qy) || cy > ly) continue;
+            if (cy < cube_first(gf.n, qy) || cy > ly) continue;
             for (int cx = I - 1; cx <= I; cx++) {
-                if (cx < cube_first(qx) || cx > lx) continue;
+                if (cx < cube_first(gf.m, qx) || cx > lx) continue;
                 for (int dz = 0; dz < 2; dz++) {
                     if (dz && !has_upper(cz, gf.o, qz)) continue;
                     bool zsn = snapped(cz, gf.o, qz);
@@ -245,6 +245,127 @@ static __global__ void __launch_bounds__(kRatSmallBlock, 4) k_rat_fill_small(Lev
         }
     }
     if (mine) Ac[((long)gc.colour(I, J, K) * 27 + lane) * gc.Nc + gc.cidx(I, J, K)] = acc;
+}
+
+// k_rat_fill restructured for throughput on non-periodic levels: one thread
+// per (coarse point, coarse stencil slot) -- the accumulator of that slot in
+// a register -- and the fine stencils and boxes the coarse points read staged
+// in shared memory once per CTA instead of per thread.  A CTA covers kRtX
+// coarse points of one coarse row (threads: slot-major, so a warp is 32
+// consecutive coarse points with the same slot and the same control flow in
+// the interior) and walks up kRtKC coarse planes; the fine points that
+// transfer to them lie in fine rows 2J-1..2J+1 and fine x 2*I0-1..2*I0+63,
+// held as a ring of three fine planes.  Each accumulator receives k_rat_fill's
+// terms in k_rat_fill's order (fine points in cube scan order, each fine
+// point's terms in A_red's order), so the coarse stencils are the same bit
+// for bit.
+constexpr int kRtX = 32;
+constexpr int kRtThreads = kRtX * 27;
+constexpr int kRtKC = 16;
+constexpr int kRtFX = 2 * kRtX + 2;  // 65 fine x values, padded
+constexpr int kRtPA = 27 * 3 * kRtFX;  // doubles per staged fine plane
+constexpr int kRtPS = 3 * kRtFX * 8;   // box bytes per staged fine plane
+constexpr size_t kRtSmem = 3 * (kRtPA * sizeof(double) + kRtPS);
+
+static __global__ void __launch_bounds__(kRtThreads, 1) k_rat_tile(LevelGeom gf, LevelGeom gc,
+                                                                   const double* __restrict__ Af,
+                                                                   const int8_t* __restrict__ Sf,
+                                                                   double* __restrict__ Ac) {
+    extern __shared__ double rsm[];
+    double* As = rsm;
+    int8_t* Ss = reinterpret_cast<int8_t*>(rsm + 3 * kRtPA);
+    const int I0 = blockIdx.x * kRtX, J = blockIdx.y, K0 = blockIdx.z * kRtKC;
+    const int K1 = K0 + kRtKC < gc.o ? K0 + kRtKC : gc.o;
+    const int fi0 = 2 * I0 - 1, fj0 = 2 * J - 1;
+    const int tid = threadIdx.x;
+    const int slot = tid / kRtX;
+    const int I = I0 + tid % kRtX;
+    auto stage = [&](int fk) {
+        if (fk < 0 || fk >= gf.o) return;
+        double* A = As + (fk % 3) * kRtPA;
+        int8_t* S = Ss + (fk % 3) * kRtPS;
+        for (int e = tid; e < 27 * 3 * 65; e += kRtThreads) {
+            int fx = e % 65, t2 = e / 65, fy = t2 % 3, q = t2 / 3;
+            int fi = fi0 + fx, fj = fj0 + fy;
+            if (fi < 0 || fi >= gf.m || fj < 0 || fj >= gf.n) continue;
+            A[(q * 3 + fy) * kRtFX + fx] = __ldg(Af + gf.ai(fi, fj, fk, q));
+        }
+        for (int e = tid; e < 3 * 65 * 6; e += kRtThreads) {
+            int u = e % 6, t2 = e / 6, fx = t2 % 65, fy = t2 / 65;
+            int fi = fi0 + fx, fj = fj0 + fy;
+            if (fi < 0 || fi >= gf.m || fj < 0 || fj >= gf.n) continue;
+            S[(fy * kRtFX + fx) * 8 + u] = Sf[6 * gf.pi(fi, fj, fk) + u];
+        }
+    };
+    const int vi = I + slot % 3 - 1, vj = J + (slot / 3) % 3 - 1;
+    const int lx = cube_last(gf.m), ly = cube_last(gf.n), lz = cube_last(gf.o);
+    stage(2 * K0 - 1);
+    for (int K = K0; K < K1; K++) {
+        stage(2 * K);
+        stage(2 * K + 1);
+        __syncthreads();
+        const int vk = K + slot / 9 - 1;
+        if (I < gc.m) {
+            double acc = 0.0;
+            for (int cz = K - 1; cz <= K; cz++) {
+                if (cz < 0 || cz > lz) continue;
+                for (int cy = J - 1; cy <= J; cy++) {
+                    if (cy < 0 || cy > ly) continue;
+                    for (int cx = I - 1; cx <= I; cx++) {
+                        if (cx < 0 || cx > lx) continue;
+                        for (int dz = 0; dz < 2; dz++) {
+                            if (dz && !has_upper(cz, gf.o)) continue;
+                            bool zsn = snapped(cz, gf.o);
+                            if (tweight(cz, dz, K, zsn) == 0.0) continue;
+                            for (int dy = 0; dy < 2; dy++) {
+                                if (dy && !has_upper(cy, gf.n)) continue;
+                                bool ysn = snapped(cy, gf.n);
+                                if (tweight(cy, dy, J, ysn) == 0.0) continue;
+                                for (int dx = 0; dx < 2; dx++) {
+                                    if (dx && !has_upper(cx, gf.m)) continue;
+                                    bool xsn = snapped(cx, gf.m);
+                                    if (tweight(cx, dx, I, xsn) == 0.0) continue;
+                                    double fac = ((dx && !xsn) ? 0.5 : 1.0) * ((dy && !ysn) ? 0.5 : 1.0) *
+                                                 ((dz && !zsn) ? 0.5 : 1.0);
+                                    int ti = 2 * cx + dx, tj = 2 * cy + dy, tk = 2 * cz + dz;
+                                    const int fx = ti - fi0, fy = tj - fj0;
+                                    const int8_t* fs = Ss + (tk % 3) * kRtPS + (fy * kRtFX + fx) * 8;
+                                    int B[6] = {fs[0] + ti, fs[1] + ti, fs[2] + tj, fs[3] + tj, fs[4] + tk, fs[5] + tk};
+                                    int St[6] = {B[0], B[1], B[2], B[3], B[4], B[5]};
+                                    grid_map(St[0], St[1], gf.m);
+                                    grid_map(St[2], St[3], gf.n);
+                                    grid_map(St[4], St[5], gf.o);
+                                    if (vi < St[0] || vi >= St[1] || vj < St[2] || vj >= St[3] || vk < St[4] ||
+                                        vk >= St[5])
+                                        continue;
+                                    const double* row = As + (tk % 3) * kRtPA + fy * kRtFX + fx;
+                                    int lk, uk, ck = igrid_map(lk, uk, B[4], B[5], vk, gf.o);
+                                    int lj, uj, cj = igrid_map(lj, uj, B[2], B[3], vj, gf.n);
+                                    int li, ui, ci = igrid_map(li, ui, B[0], B[1], vi, gf.m);
+                                    double At = 0.0;
+                                    for (int kk = lk; kk < uk; kk++) {
+                                        double kfac = kk == ck ? 1.0 : 0.5;
+                                        for (int jj = lj; jj < uj; jj++) {
+                                            double jkfac = jj == cj ? kfac : 0.5 * kfac;
+                                            for (int ii = li; ii < ui; ii++) {
+                                                int q = (ii - ti + 1) + 3 * (jj - tj + 1) + 9 * (kk - tk + 1);
+                                                double term = __dmul_rn(__dmul_rn(0.125, row[q * 3 * kRtFX]),
+                                                                        ii == ci ? jkfac : 0.5 * jkfac);
+                                                At = __dadd_rn(At, term);
+                                            }
+                                        }
+                                    }
+                                    acc = __dadd_rn(acc, __dmul_rn(At, fac));
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            Ac[((long)gc.colour(I, J, K) * 27 + slot) * gc.Nc + gc.cidx(I, J, K)] = acc;
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -548,6 +669,121 @@ static __global__ void __launch_bounds__(1024) k_lu_band(double* __restrict__ M,
                 M[a] = __dsub_rn(M[a], __dmul_rn(sL[ii], u));
             }
         }
+        __syncthreads();
+    }
+}
+
+// The same factorisation with the active window in shared memory.  At step
+// j only rows j..j+kl and columns j..j+kl+ku can change (above), so the
+// kernel keeps that window -- (kl+1) x (kl+ku+1) doubles, rows and columns
+// stored circularly by index modulo the window size -- and streams the
+// matrix through it: a row or column enters from the dense matrix the step
+// before it is first needed (no earlier step has touched it) and leaves when
+// its last entry is final (column j and row j after step j).  The row
+// interchange of step j also swaps the two rows' multipliers left of
+// column j, which lie in the dense matrix: row_first[i] tracks the first
+// column at which the row now at position i holds a multiplier (rows carry
+// it when they are interchanged), so the swap covers exactly the columns
+// where either row can be non-zero.  Every entry receives the operations of
+// k_lu_band in the same order, so the factors and pivots are identical.
+constexpr size_t kLuWindowSmemMax = 220 * 1024;
+__host__ __device__ inline size_t lu_window_smem(int n, int kl, int ku) {
+    return sizeof(double) * ((size_t)(kl + 1) * (kl + ku + 1) + kl + (kl + ku) + 64) + sizeof(int) * ((size_t)n + 64);
+}
+
+static __global__ void __launch_bounds__(1024) k_lu_window(double* __restrict__ M, int n, int kl, int ku,
+                                                           int* __restrict__ piv, int* __restrict__ info) {
+    extern __shared__ double smem[];
+    const int RW = kl + 1, CW = kl + ku + 1;
+    double* W = smem;
+    double* sL = W + (size_t)RW * CW;
+    double* sU = sL + kl;
+    double* wv = sU + (kl + ku);
+    int* rowfirst = reinterpret_cast<int*>(wv + 64);
+    int* wi = rowfirst + n;
+    int* s_p = wi + 32;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+    auto at = [&](int i, int c) -> double& { return W[(i % RW) * CW + (c % CW)]; };
+    if (tid == 0) info[0] = 0;
+    for (int e = tid; e < RW * CW; e += blockDim.x) {
+        int r = e / CW, c = e % CW;
+        W[e] = (r < n && c < n) ? M[r + (long)c * n] : 0.0;
+    }
+    for (int i = tid; i < n; i += blockDim.x) rowfirst[i] = i > kl ? i - kl : 0;
+    __syncthreads();
+    for (int j = 0; j < n; j++) {
+        const int R = min(n - 1, j + kl) - j;
+        const int C = min(n - 1, j + kl + ku) - j;
+        double bv = -1.0;
+        int bi = n;
+        for (int i = j + tid; i <= j + R; i += blockDim.x) lu_better(fabs(at(i, j)), i, bv, bi);
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            lu_better(ov, oi, bv, bi);
+        }
+        if (lane == 0) { wv[w] = bv; wi[w] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 1; q < nw; q++) lu_better(wv[q], wi[q], wv[0], wi[0]);
+            int p = wi[0] < n ? wi[0] : j;
+            *s_p = p;
+            piv[j] = p + 1;
+        }
+        __syncthreads();
+        const int p = *s_p;
+        const double apj = at(p, j);
+        if (apj != 0.0) {
+            if (p != j) {
+                for (int c = j + tid; c <= j + C; c += blockDim.x) {
+                    double a = at(j, c);
+                    at(j, c) = at(p, c);
+                    at(p, c) = a;
+                }
+                const int lo = min(rowfirst[j], rowfirst[p]);
+                for (int c = lo + tid; c < j; c += blockDim.x) {
+                    double a = M[j + (long)c * n], b2 = M[p + (long)c * n];
+                    M[j + (long)c * n] = b2;
+                    M[p + (long)c * n] = a;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    int t = rowfirst[j];
+                    rowfirst[j] = rowfirst[p];
+                    rowfirst[p] = t;
+                }
+            }
+            __syncthreads();
+            const double r = 1.0 / at(j, j);
+            for (int i = tid; i < R; i += blockDim.x) {
+                double v = __dmul_rn(at(j + 1 + i, j), r);
+                at(j + 1 + i, j) = v;
+                sL[i] = v;
+            }
+        } else {
+            if (tid == 0 && info[0] == 0) info[0] = j + 1;
+            for (int i = tid; i < R; i += blockDim.x) sL[i] = at(j + 1 + i, j);
+        }
+        for (int k = tid; k < C; k += blockDim.x) sU[k] = at(j, j + 1 + k);
+        __syncthreads();
+        for (int q = tid; q < R * C; q += blockDim.x) {
+            int ii = q % R, kk = q / R;
+            double u = sU[kk];
+            if (u != 0.0) {
+                double& a = at(j + 1 + ii, j + 1 + kk);
+                a = __dsub_rn(a, __dmul_rn(sL[ii], u));
+            }
+        }
+        // Column j (rows j..j+R) and row j (columns j+1..j+C) are final.
+        for (int i = tid; i <= R; i += blockDim.x) M[(j + i) + (long)j * n] = at(j + i, j);
+        for (int k = tid; k < C; k += blockDim.x) M[j + (long)(j + 1 + k) * n] = sU[k];
+        __syncthreads();
+        // Slide: row j+kl+1 takes row j's slots, column j+kl+ku+1 column j's.
+        const int nr = j + kl + 1, nc = j + kl + ku + 1;
+        if (nr < n)
+            for (int c = j + 1 + tid; c <= nc && c < n; c += blockDim.x) at(nr, c) = M[nr + (long)c * n];
+        if (nc < n)
+            for (int i = j + 1 + tid; i < nr && i < n; i += blockDim.x) at(i, nc) = M[i + (long)nc * n];
         __syncthreads();
     }
 }

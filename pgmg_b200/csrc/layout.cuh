@@ -121,18 +121,24 @@ __host__ __device__ inline int slab_lo(const LevelGeom& g, int s, int slabs) {
 // exists; the upper point 2C+1 exists unless C is the last cube of an odd
 // axis; on an even axis the last cube's upper point (ma-1) "snaps" onto
 // coarse C+1 with weight 1 (mask bits 4/32/256).
-// A periodic axis (p; even ma, coarse size ma/2, region.cc:14) has cubes
-// C = -1..ma/2-1, all with both points and none snapped: cube -1 is the image
-// of cube ma/2-1, whose upper point ma-1 sits just below fine point 0 and
-// also transfers to coarse 0.  Indices of such images are unwrapped here and
-// wrapped only to address memory (wrap()).
-__host__ __device__ inline int cube_first(bool p) { return p ? -1 : 0; }
+// An even periodic axis (p, even ma; coarse size ma/2, region.cc:14) has
+// cubes C = -1..ma/2-1, all with both points and none snapped: cube -1 is
+// the image of cube ma/2-1, whose upper point ma-1 sits just below fine
+// point 0 and also transfers to coarse 0.  Indices of such images are
+// unwrapped here and wrapped only to address memory (wrap()).
+// An odd periodic axis (coarse size (ma+1)/2) transfers like an odd
+// non-periodic one: coarse (ma-1)/2 sits on fine ma-1, the next coarse point
+// across the seam is coarse 0 on fine ma = 0, and no fine point lies between
+// them (igrid_map's odd periodic branch, region.cc:1236-1243); only the
+// stencils wrap around.
+__host__ __device__ inline bool even_prd(int ma, bool p) { return p && !(ma & 1); }
+__host__ __device__ inline int cube_first(int ma, bool p) { return even_prd(ma, p) ? -1 : 0; }
 __host__ __device__ inline int cube_last(int ma, bool p = false) {
-    if (p) return (ma >> 1) - 1;
+    if (even_prd(ma, p)) return (ma >> 1) - 1;
     int sm = (ma + 2) >> 1;
     return (ma & 1) ? sm - 1 : sm - 2;
 }
-__host__ __device__ inline bool has_upper(int C, int ma, bool p = false) { return p || 2 * C + 1 < ma; }
+__host__ __device__ inline bool has_upper(int C, int ma, bool p = false) { return even_prd(ma, p) || 2 * C + 1 < ma; }
 __host__ __device__ inline bool snapped(int C, int ma, bool p = false) { return !p && !(ma & 1) && C == cube_last(ma); }
 __host__ __device__ inline int wrap(int v, int size, bool p) {
     return p ? (v < 0 ? v + size : (v >= size ? v - size : v)) : v;
@@ -161,11 +167,21 @@ __host__ __device__ inline void grid_map(int& lo, int& hi, int ma, bool p = fals
 }
 
 // igrid_map with the crop to the stencil box (region.cc:1231-1259): the fine
-// range a coarse index gathers from, and its coincident fine index.  Periodic
-// axes here are even (coarse index i <-> fine 2i, range [2i-1, 2i+2)).
+// range a coarse index gathers from, and its coincident fine index.  On an
+// even periodic axis coarse i <-> fine 2i with range [2i-1, 2i+2); on an odd
+// one the coarse images i < 0 and i >= (ma+1)/2 sit one fine point closer
+// (the short cell at the seam) and ranges end at the seam.
 __host__ __device__ inline int igrid_map(int& lo, int& hi, int blo, int bhi, int i, int ma, bool p = false) {
-    int j = i << 1;
-    if (p) { lo = j - 1; hi = j + 2; }
+    int j = i * 2;
+    if (p && (ma & 1)) {
+        int llo, hhi;
+        if (j < 0) { j += 1; llo = -ma; hhi = 0; }
+        else if (j >= ma) { j -= 1; llo = ma; hhi = 2 * ma; }
+        else { llo = 0; hhi = ma; }
+        lo = j == llo ? llo : j - 1;
+        hi = j == hhi - 1 ? hhi : j + 2;
+    }
+    else if (p) { lo = j - 1; hi = j + 2; }
     else if (ma & 1) { lo = j == 0 ? 0 : j - 1; hi = j == ma - 1 ? ma : j + 2; }
     else if (j == ma) { lo = ma - 1; hi = ma; j = ma - 1; }
     else { lo = j == 0 ? 0 : j - 1; hi = j == ma - 2 ? ma - 1 : j + 2; }

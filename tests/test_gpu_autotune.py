@@ -168,3 +168,57 @@ def test_autotune_cache_file(tmp_path):
     # Another precision is a different entry.
     C = make((65, 49, 33), P.MIXED)
     assert "cached" not in C.autotune(cache=cache)
+
+
+@pytest.mark.parametrize("mno", [(65, 65, 65), (41, 33, 18), (66, 34, 20), (129, 97, 65), (20, 33, 9)])
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_fused_restriction_bitwise(mno, precision):
+    """The restriction that computes its residuals in shared memory gives the
+    coarse sources of the residual pass plus restriction bit for bit, on odd,
+    even and anisotropic grids (tiles cut at every edge), and the same
+    solves."""
+    A = make(mno, precision)
+    A.set_option(P.OPT_FUSED_RESTRICT, 0)
+    rng = np.random.default_rng(6)
+    xs = [rng.standard_normal(A.npts(l - 1)) for l in range(1, A.nlevels)]
+    ref = []
+    for l in range(1, A.nlevels):
+        A.set_x(l - 1, xs[l - 1])
+        A.restriction(l)
+        ref.append(A.get_r(l))
+    A.clear_x(0)
+    A.solve(1e-10, 100, 1)
+    xa = A.get_x(0)
+    for variant in (1, 2):
+        B = make(mno, precision)
+        B.set_option(P.OPT_FUSED_RESTRICT, variant)
+        for l in range(1, B.nlevels):
+            B.set_x(l - 1, xs[l - 1])
+            B.restriction(l)
+            assert np.array_equal(B.get_r(l), ref[l - 1]), (variant, l)
+            assert not np.any(B.get_x(l))
+        B.clear_x(0)
+        B.solve(1e-10, 100, 1)
+        assert np.array_equal(B.get_x(0), xa), variant
+
+
+@pytest.mark.parametrize("mno", [(33, 33, 33), (65, 65, 65), (20, 33, 9), (41, 41, 41), (16, 17, 18)])
+@pytest.mark.parametrize("coarse", [P.COARSE_LU_EXACT, P.COARSE_LU])
+def test_lu_window_same_factors(mno, coarse):
+    """The coarse LU factorised in a shared-memory band window gives the
+    one-block device-memory factorisation's factors and pivots bit for bit:
+    the reference-order coarse solve and the explicit inverse (and so the
+    V-cycles that use them) agree exactly."""
+    coef, S, r = q1_problem(*mno, sigma=1.0, seed=sum(mno) + 3)
+    hs = []
+    for win in (0, 1):
+        G = P.Multigrid(*mno, coarse=coarse, smoother=P.SMOOTH_LEX)
+        G.set_option(P.OPT_LU_WINDOW, win)
+        G.setup_matrices(coef, S)
+        G.setup_fields(r)
+        assert G.lu_enabled
+        hs.append(G)
+    for _ in range(3):
+        for G in hs:
+            G.v_cycle(0)
+        assert np.array_equal(hs[0].get_x(0), hs[1].get_x(0))

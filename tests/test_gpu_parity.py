@@ -316,3 +316,18 @@ def test_sweep_count_options():
     G2, _ = make(mno, coarse=P.COARSE_GS, smoother=P.SMOOTH_MC8)
     G2.v_cycle(0)
     assert not np.array_equal(G.get_x(0), G2.get_x(0))
+
+
+@pytest.mark.parametrize("mno", [(65, 65, 65), (81, 40, 66), (66, 50, 41), (97, 33, 70)])
+def test_rat_large_levels_bitwise(mno):
+    """Coarse levels of more than 20,000 points (built by the tiled Galerkin
+    kernel, one thread per coarse point and stencil slot): boxes and
+    stencils bit for bit the oracle's, on odd, even and mixed sizes whose
+    tiles are cut at every edge."""
+    G, prob = make(mno)
+    O = oracle_for(mno, prob, G.lu_enabled)
+    assert G.nlevels == O.nlevels
+    assert G.dims(1)[0] * G.dims(1)[1] * G.dims(1)[2] > 20000
+    for l in range(G.nlevels):
+        assert np.array_equal(G.get_boxes(l), O.get_S(l)), l
+        assert np.array_equal(G.get_coef(l), O.get_A27(l)), l

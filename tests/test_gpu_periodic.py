@@ -3,6 +3,10 @@ branches region.cc:1202-1208, 1233-1242, ghost wrap region.cc:1338-1469):
 the CUDA path against the reference itself (oracle/_ref, built with the
 periodic ghost exchange of its single-rank MPI shim).
 
+Odd periodic sizes are included, on the finest level and on levels above the
+coarsest: their transfers take igrid_map's odd periodic branch, and such a
+level is swept lexicographically by the 8-colour smoother too.
+
 The reference adds the contributions that cross a periodic boundary through
 its restriction and RAT strips after the local ones, so sums at those points
 associate differently here.  Tolerances (relative to the largest entry):
@@ -21,7 +25,12 @@ from tests.helpers import periodic_problem, relerr
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")]
 
 CASES = [((16, 12, 18), (True, False, True)), ((16, 16, 16), (True, True, True)),
-         ((32, 20, 16), (False, True, True)), ((24, 24, 40), (True, True, False))]
+         ((32, 20, 16), (False, True, True)), ((24, 24, 40), (True, True, False)),
+         # odd periodic sizes above the coarsest level (region.cc:1202-1208,
+         # 1236-1243): 50 -> 25 -> 13; 30 -> 15 and 18 -> 9; 25 on level 0;
+         # 44 -> 22 -> 11 -> 6 on all three axes
+         ((50, 16, 16), (True, False, False)), ((30, 18, 18), (True, False, True)),
+         ((25, 16, 16), (True, False, False)), ((44, 44, 44), (True, True, True))]
 
 
 def make(mno, prd, precision=P.FP64, smoother=P.SMOOTH_LEX, coarse=P.COARSE_LU_EXACT, seed=3):
@@ -121,7 +130,8 @@ def test_periodic_mc8_contraction(mno, prd):
     assert fg <= 1.05 * fr
 
 
-def test_periodic_odd_level_rejected():
-    with pytest.raises(P.PgmgError) as e:
-        P.Multigrid(44, 44, 44, prd=(True, True, True))  # 44 -> 22 -> 11 (odd, smoothed) -> 6
-    assert e.value.status == 11
+def test_periodic_odd_levels_planned():
+    """A periodic axis that turns odd on a smoothed level is planned as the
+    reference plans it (coarse size (m+1)>>1, region.cc:14)."""
+    G = P.Multigrid(44, 44, 44, prd=(True, True, True))
+    assert [G.dims(l) for l in range(G.nlevels)] == [(44, 44, 44), (22, 22, 22), (11, 11, 11), (6, 6, 6)]
