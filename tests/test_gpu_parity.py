@@ -318,7 +318,7 @@ def test_sweep_count_options():
     assert not np.array_equal(G.get_x(0), G2.get_x(0))
 
 
-@pytest.mark.parametrize("mno", [(65, 65, 65), (81, 40, 66), (66, 50, 41), (97, 33, 70)])
+@pytest.mark.parametrize("mno", [(65, 65, 65), (81, 40, 66), (66, 58, 49), (97, 33, 70)])
 def test_rat_large_levels_bitwise(mno):
     """Coarse levels of more than 20,000 points (built by the tiled Galerkin
     kernel, one thread per coarse point and stencil slot): boxes and
