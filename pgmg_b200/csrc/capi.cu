@@ -296,9 +296,7 @@ pgmg_status fused_restrict(pgmg_handle* h, Level& F, Level& Cl, View<T>& vf, Vie
     const LevelGeom& gc = Cl.g;
     dim3 grid((unsigned)((gc.m + Tile::tx - 1) / Tile::tx), (unsigned)((gc.n + Tile::ty - 1) / Tile::ty),
               (unsigned)((gc.o + Tile::kc - 1) / Tile::kc));
-    const size_t sm = Tile::template smem<T>();
-    if (sm > 48 * 1024)
-        CK(cudaFuncSetAttribute(k_resrestrict<T, Tile>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const size_t sm = Tile::template smem<T>();  // limit set in prepare_device_kernels
     h->launches++;
     CK(launch_k_smem(h->stream, h->pdl, grid, dim3(Tile::threads), sm, k_resrestrict<T, Tile>, F.g, gc,
                      (const T*)vf.x, (const T*)vf.r, (const T*)vf.A, vc.r, vc.x));
@@ -397,8 +395,14 @@ pgmg_status launch_coarse(pgmg_handle* h, int first, int mode) {
         // whose copy does not fit sweep from global memory).
         long need = 0;
         for (int l = h->coarse_first; l < h->nl; l++) {
-            // The colour-major x copy and the staged stencils, for levels where both fit.
-            long b = shared_copy(h->L[l].g, h->cluster_size).bytes((int)sizeof(T));
+            const LevelGeom& g = h->L[l].g;
+            // The x copy and the staged stencils, for levels where both fit;
+            // else the level's z-plane windows (c_sweeps_window), where
+            // every CTA's points fit in one pass of its threads.
+            long b = shared_copy(g, h->cluster_size).bytes((int)sizeof(T));
+            long nc = (long)g.M2 * g.N2 * g.O2;
+            if (b > kCoarseXsMax && (nc + h->cluster_size - 1) / h->cluster_size <= kClusterThreads)
+                b = window_bytes(g, h->cluster_size, (int)sizeof(T));
             if (b <= kCoarseXsMax && b > need) need = b;
         }
         cfg.dynamicSmemBytes = (size_t)need;
@@ -660,8 +664,8 @@ pgmg_status lu_setup(pgmg_handle* h) {
         if (kb > (int)n - 1) kb = (int)n - 1;
         size_t wsm = lu_window_smem((int)n, kb, kb);
         if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax) {
-            // The active band window in shared memory (same factors).
-            CK(cudaFuncSetAttribute(k_lu_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+            // The active band window in shared memory (same factors; the
+            // limit is set in prepare_device_kernels).
             k_lu_window<<<1, 1024, wsm, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
         } else {
             k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
@@ -696,6 +700,42 @@ void guide_update(pgmg_handle* h, int extras) {
     }
     h->iter += diter;
     if (h->iter < h->period) h->iter = 2 * h->period - 1;
+}
+
+// Once per device, before the first handle on it does any work: the
+// dynamic shared-memory limits of the kernels that need more than 48 KiB,
+// and a query of every set-up kernel's attributes, which also loads it.
+// With lazy module loading a kernel is otherwise loaded at its first use,
+// and a first use on one thread (a server's set-up thread) while another
+// thread captures a CUDA graph invalidates that capture.
+pgmg_status prepare_device_kernels(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64) return PGMG_ERR_ARG;
+    if (done[device]) return PGMG_OK;
+    bool ok = true;
+    ok = ok && cudaFuncSetAttribute(k_lu_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLuWindowSmemMax) ==
+                   cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_resrestrict<double, RrLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)RrLarge::smem<double>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_resrestrict<float, RrLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)RrLarge::smem<float>()) == cudaSuccess;
+    cudaFuncAttributes fa;
+    const void* setup_kernels[] = {(const void*)k_lu_build,       (const void*)k_lu_band,
+                                   (const void*)k_lu_inverse,     (const void*)k_rat_bounds,
+                                   (const void*)k_rat_fill,       (const void*)k_rat_fill_small,
+                                   (const void*)k_assemble_q1,    (const void*)k_rhs_uniform,
+                                   (const void*)k_resrestrict<double, RrSmall>,
+                                   (const void*)k_resrestrict<float, RrSmall>};
+    for (const void* k : setup_kernels) ok = ok && cudaFuncGetAttributes(&fa, k) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        return PGMG_ERR_CUDA;
+    }
+    done[device] = true;
+    return PGMG_OK;
 }
 
 bool is_device_ptr(const void* p) {
@@ -743,6 +783,10 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
         cudaSetDevice(dims->device);
     }
     cudaGetDevice(&h->device);
+    if (prepare_device_kernels(h->device) != PGMG_OK) {
+        delete h;
+        return PGMG_ERR_CUDA;
+    }
     LevelGeom g[kMaxLevels];
     h->nl = plan_levels(*dims, g);
     for (int l = 0; l < h->nl; l++) h->L[l].g = g[l];
@@ -1089,7 +1133,6 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
             k_rat_fill_small<<<nblk(Cl.g.npts * 32, kRatSmallBlock), kRatSmallBlock, 0, h->stream>>>(F.g, Cl.g, F.A64,
                                                                                                    F.S, Cl.A64);
         } else if (!F.g.prd) {
-            CK(cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem));
             dim3 grid((unsigned)((Cl.g.m + kRtX - 1) / kRtX), (unsigned)Cl.g.n, (unsigned)((Cl.g.o + kRtKC - 1) / kRtKC));
             k_rat_tile<<<grid, kRtThreads, kRtSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         } else {

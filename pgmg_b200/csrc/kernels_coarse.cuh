@@ -240,6 +240,112 @@ __device__ __noinline__ void c_sweeps_shared(const LevelGeom g, T* x, const T* r
     cluster_sync();
 }
 
+// Halo'd z planes [lo, hi] of a level that CTA `rank` of a `csize`-CTA
+// cluster needs when it owns colour points [rank*chunk, (rank+1)*chunk) of
+// every colour (c_sweeps_shared's ownership): the fine planes of its points
+// and one more on each side.  hi < lo when it owns none.
+__host__ __device__ inline void win_planes(const LevelGeom& g, int rank, int csize, int& lo, int& hi) {
+    const long nc = (long)g.M2 * g.N2 * g.O2, chunk = (nc + csize - 1) / csize, pl = (long)g.M2 * g.N2;
+    const long p0 = (long)rank * chunk, p1 = ((long)(rank + 1) * chunk < nc ? (long)(rank + 1) * chunk : nc) - 1;
+    if (p0 >= nc) {
+        lo = 0;
+        hi = -1;
+        return;
+    }
+    const int k2lo = (int)(p0 / pl), k2hi = (int)(p1 / pl);
+    lo = 2 * k2lo;                                      // fine plane 2*k2lo - 1, halo'd
+    hi = 2 * k2hi + 3 < g.o + 1 ? 2 * k2hi + 3 : g.o + 1;  // fine plane 2*k2hi + 2, halo'd
+}
+// Bytes of the largest window of a level over the CTAs of the cluster.
+__host__ __device__ inline long window_bytes(const LevelGeom& g, int csize, int tsize) {
+    long w = 0;
+    for (int d = 0; d < csize; d++) {
+        int lo, hi;
+        win_planes(g, d, csize, lo, hi);
+        long b = (long)(hi - lo + 1) * g.mx * g.my * tsize;
+        if (b > w) w = b;
+    }
+    return w;
+}
+
+// The sweeps of a level whose full shared copy (c_sweeps_shared) does not
+// fit, with x from shared memory all the same: each CTA holds only the window
+// of halo'd z planes its own points and their neighbours lie in (win_planes;
+// points owned as in c_sweeps_shared), loaded from global memory at the
+// start.  A new value goes with st.shared::cluster stores into the window of
+// every CTA that holds its plane, ordered by the release/acquire cluster
+// barrier of the pass.  The stencil, source and diagonal reciprocal of a
+// thread's next colour are fetched from L2 into registers between the halves
+// of that barrier, as in c_sweeps_owned.  At the end each owner writes its
+// points back.  Same arithmetic as c_sweeps_owned.
+template <class T>
+__device__ __noinline__ void c_sweeps_window(const LevelGeom g, T* x, const T* r, const T* A, int sweeps, int mode,
+                                             T* sm, int rank, int csize) {
+    const long nc = (long)g.M2 * g.N2 * g.O2;
+    const int chunk = (int)((nc + csize - 1) / csize);
+    const int p = rank * chunk + (int)threadIdx.x;
+    const bool have = (int)threadIdx.x < chunk && p < nc;
+    int i2 = 0, j2 = 0, k2 = 0;
+    if (have) decode_colour(g, p, i2, j2, k2);
+    // Shared-memory indexes fit in 32 bits (a window is at most kCoarseXsMax bytes).
+    const int mxi = (int)g.mx, szi = (int)(g.mx * g.my);
+    int lo, hi;
+    win_planes(g, rank, csize, lo, hi);
+    const int wbase = lo * szi;
+    for (int e = threadIdx.x; e < (hi - lo + 1) * szi; e += blockDim.x) sm[e] = __ldcg(x + wbase + e);
+    const int xc0 = (int)g.xi(2 * i2, 2 * j2, 2 * k2);
+    auto valid = [&](int col) {
+        return have && 2 * i2 + (col & 1) < g.m && 2 * j2 + ((col >> 1) & 1) < g.n && 2 * k2 + (col >> 2) < g.o;
+    };
+    auto at = [&](int col) { return xc0 + (col & 1) + ((col >> 1) & 1) * mxi + (col >> 2) * szi; };
+    const int per = mode ? 16 : 8, total = sweeps * per;
+    auto colour_at = [&](int st) {
+        int cc = st % per;
+        return colour_seq(cc < 8 ? cc : 15 - cc);
+    };
+    T a[27];
+    T rv = T(0), ainv = T(1);
+    auto fetch = [&](int col) {
+        if (!valid(col)) return;
+        const T* Ap = A + (long)col * 27 * g.Nc + p;
+#pragma unroll
+        for (int q = 0; q < 27; q++) a[q] = __ldg(Ap + q * g.Nc);
+        rv = __ldcg(r + (long)col * g.Nc + p);
+        ainv = T(1) / a[13];
+    };
+    const uint32_t base = smem_u32(sm);
+    if (total > 0) fetch(colour_at(0));
+    // Every window is loaded before any CTA writes into another's.
+    cluster_sync();
+    for (int st = 0; st < total; st++) {
+        int col = colour_at(st);
+        if (valid(col)) {
+            const int gi = at(col);
+            const T* xp = sm + (gi - wbase);
+            T acc = T(0);
+#pragma unroll
+            for (int q = 0; q < 27; q++) {
+                if (q == 13) continue;
+                acc = madd<true, T>(acc, a[q], xp[(q % 3 - 1) + mxi * ((q / 3) % 3 - 1) + szi * (q / 9 - 1)]);
+            }
+            const T v = mul_rn<T>(sub_rn<T>(rv, acc), ainv);
+            const int hz = gi / szi;
+            for (int d = 0; d < csize; d++) {
+                int dl, dh;
+                win_planes(g, d, csize, dl, dh);
+                if (hz < dl || hz > dh) continue;
+                st_cl(cl_map(base + (uint32_t)(gi - dl * szi) * (uint32_t)sizeof(T), (uint32_t)d), v);
+            }
+        }
+        cl_arrive();
+        if (st + 1 < total) fetch(colour_at(st + 1));
+        cl_wait();
+    }
+    for (int col = 0; col < 8; col++)
+        if (valid(col)) x[at(col)] = sm[at(col) - wbase];
+    cluster_sync();
+}
+
 template <class T>
 __device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, const T* A, int sweeps, int mode,
                                          long long budget, int tid, int nth, T* xs, int rank, int csize) {
@@ -247,6 +353,9 @@ __device__ __forceinline__ void c_sweeps(const LevelGeom g, T* x, const T* r, co
     if (S == 1 && (long)g.M2 * g.N2 * g.O2 <= nth) {
         if (xs && shared_copy(g, csize).bytes((int)sizeof(T)) <= (long)dyn_smem_bytes())
             c_sweeps_shared<T>(g, x, r, A, sweeps, mode, xs, rank, csize);
+        else if (xs && (long)((g.M2 * g.N2 * g.O2 + csize - 1) / csize) <= (long)blockDim.x &&
+                 window_bytes(g, csize, (int)sizeof(T)) <= (long)dyn_smem_bytes())
+            c_sweeps_window<T>(g, x, r, A, sweeps, mode, xs, rank, csize);
         else
             c_sweeps_owned<T>(g, x, r, A, sweeps, mode, tid);
         return;

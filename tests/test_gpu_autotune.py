@@ -134,10 +134,13 @@ def test_gs_prefetch_bitwise(precision, pdl):
 
 
 @pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
-@pytest.mark.parametrize("mno,first", [((65, 65, 65), 2), ((97, 81, 49), 2), ((129, 129, 129), 3)])
+@pytest.mark.parametrize("mno,first", [((65, 65, 65), 2), ((97, 81, 49), 2), ((129, 129, 129), 3),
+                                       ((65, 65, 65), 1), ((129, 129, 129), 2), ((66, 60, 50), 1)])
 def test_coarse_shared_bitwise(precision, mno, first):
     """The cluster coarse cycle sweeping from a shared-memory copy of each
-    level's x gives the same iterates as sweeping from global memory."""
+    level's x -- or, for a 33^3-sized level whose copy does not fit, from
+    per-CTA windows of z planes -- gives the same iterates as sweeping from
+    global memory."""
     A = make(mno, precision)
     B = make(mno, precision)
     for G in (A, B):
