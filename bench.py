@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-seq-seconds", type=float, default=60.0,
                     help="time budget of the one-request-at-a-time comparison")
+    ap.add_argument("--serve-sustained-seconds", type=float, default=30.0,
+                    help="length of the second serving run, at 80%% of the saturated throughput (0 = skip)")
     return ap.parse_args()
 
 
@@ -819,6 +821,29 @@ def run_serve(a):
     srv.close()
     del srv
     torch.cuda.empty_cache()
+    # Latency at a load the server sustains: a second open-loop stream at 80 %
+    # of the saturated throughput just measured.  Sustained means the late
+    # requests wait no longer than the early ones (the queue does not grow).
+    if a.serve_sustained_seconds > 0:
+        rate2 = 0.8 * out["value"]
+        reqs2 = poisson_requests(rate2, a.serve_sustained_seconds, seed=a.seed + 1, reuse=0.2, sizes=(65, 129, 257),
+                                 sigma=(0.5, 2.3))
+        for r in reqs2:
+            fields.get(r.shape, r.field)
+        srv = SolveServer(150e9, max_slots=64, precision=P.MIXED, fields=fields)
+        done2 = sorted(srv.run(reqs2), key=lambda r: r.arrival)
+        srv.close()
+        del srv
+        torch.cuda.empty_cache()
+        lat2 = np.array([r.latency for r in done2])
+        half = len(lat2) // 2
+        span2 = max(r.finished for r in done2) - min(r.arrival for r in done2)
+        out["sustained"] = {"rate_req_s": rate2, "requests": len(done2), "value": len(done2) / span2,
+                            "unit": "solves/s", "p50_latency_s": float(np.percentile(lat2, 50)),
+                            "p99_latency_s": float(np.percentile(lat2, 99)),
+                            "p50_first_half_s": float(np.percentile(lat2[:half], 50)) if half else None,
+                            "p50_second_half_s": float(np.percentile(lat2[half:], 50)) if half else None,
+                            "max_relres": float(max(r.relres for r in done2))}
     # The same requests one at a time (set-up when not resident, then a
     # solve), in arrival order, for at most --serve-seq-seconds.
     cache = {}
