@@ -186,18 +186,24 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           (a wait that runs out makes the solve return
  *                           PGMG_ERR_TIMEOUT); 0 = off (default).  No
  *                           counterpart in the reference.
- *   PGMG_OPT_FUSED_RESTRICT 1 or 2 = the restriction of a non-periodic level
+ *   PGMG_OPT_FUSED_RESTRICT 1 = the restriction of a non-periodic level
  *                           computes the fine residuals inside the restriction
  *                           kernel (tiles of the residual in shared memory, no
- *                           residual array in device memory; 1: tiles of 32 x 8
- *                           coarse points over 8 planes, default; 2: 32 x 16
- *                           over 16); 0 = a residual pass, then the
- *                           restriction.  Same results bit for bit.
+ *                           residual array in device memory); 0 = a residual
+ *                           pass, then the restriction (default: faster on a
+ *                           B200).  Same results bit for bit.
  *   PGMG_OPT_LU_WINDOW      1 = the coarsest level's LU factorisation keeps its
  *                           active band window in shared memory (default, where
  *                           it fits in 220 KiB); 0 = one thread block on the
  *                           dense matrix in device memory.  Same factors bit
- *                           for bit.  Takes effect at the next set-up. */
+ *                           for bit.  Takes effect at the next set-up.
+ *   PGMG_OPT_GS_TMA         8-colour levels of at least this many points (one
+ *                           slab, non-periodic) stage each colour pass's
+ *                           stencil coefficients and sources in shared memory
+ *                           with bulk copies of the Tensor Memory Accelerator,
+ *                           the stencils fetched before the pass waits for the
+ *                           previous kernel; 0 = off (default).  Same results
+ *                           bit for bit.  No counterpart in the reference. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -216,14 +222,15 @@ enum {
     PGMG_OPT_GS_PREFETCH = 15,
     PGMG_OPT_COARSE_SHARED = 16,
     PGMG_OPT_FUSED_RESTRICT = 17,
-    PGMG_OPT_LU_WINDOW = 18
+    PGMG_OPT_LU_WINDOW = 18,
+    PGMG_OPT_GS_TMA = 19
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
  * PGMG_OPT_GS_ALTERNATE, PGMG_OPT_GS_PREFETCH, PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE,
- * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT --
+ * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT, PGMG_OPT_GS_TMA --
  * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,
@@ -237,6 +244,13 @@ pgmg_status pgmg_dev_autotune(pgmg_handle *h, int reps, double *ms);
  * than the launch has, so its wait runs out (about a second) and the call
  * returns PGMG_ERR_TIMEOUT with the device usable; otherwise PGMG_OK. */
 pgmg_status pgmg_dev_grid_check(pgmg_handle *h, int level, int run_out);
+/* Self-check of the TMA colour pass's bounded mbarrier wait (no counterpart
+ * in the reference): one FP64 colour pass (the first colour) of `level`
+ * with k_gs_colour_tma; with run_out != 0 every CTA's barrier expects 16
+ * bytes more than its copies bring, so its wait runs out (about half a
+ * second, twice) and the call returns PGMG_ERR_TIMEOUT with the device
+ * usable; otherwise PGMG_OK. */
+pgmg_status pgmg_dev_tma_check(pgmg_handle *h, int level, int run_out);
 /* V-cycle profile (no counterpart in the reference): runs one V-cycle of the
  * handle's options, each stage launched on its own (no graph), with CUDA
  * events on the handle's stream between the stages, and writes the stage

@@ -39,6 +39,7 @@ OPT_GS_PREFETCH = 15
 OPT_COARSE_SHARED = 16
 OPT_FUSED_RESTRICT = 17
 OPT_LU_WINDOW = 18
+OPT_GS_TMA = 19
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -102,6 +103,7 @@ SIGNATURES = [
     ("pgmg_dev_vcycle", C.c_int, [_VP, C.c_int, C.c_int]),
     ("pgmg_dev_fmg_cycle", C.c_int, [_VP, C.c_int]),
     ("pgmg_dev_profile_vcycle", C.c_int, [_VP, C.c_int, _dp, C.c_int, C.POINTER(C.c_int)]),
+    ("pgmg_dev_tma_check", C.c_int, [_VP, C.c_int, C.c_int]),
     ("pgmg_dev_source_soln_dot", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
     ("pgmg_dev_soln_diff", C.c_int, [_VP, C.c_int, _VP, C.POINTER(C.c_double)]),
     ("pgmg_dev_l0_error", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double)]),
@@ -286,7 +288,7 @@ class Multigrid:
     TUNED_OPTIONS = {"gs_block": OPT_GS_BLOCK, "cluster_size": OPT_CLUSTER_SIZE, "cluster_first": OPT_CLUSTER_FIRST,
                      "pdl": OPT_PDL, "grid_max": OPT_GRID_MAX, "gs_vector": OPT_GS_VECTOR,
                      "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH,
-                     "fused_restrict": OPT_FUSED_RESTRICT}
+                     "fused_restrict": OPT_FUSED_RESTRICT, "gs_tma": OPT_GS_TMA}
 
     def autotune(self, reps: int = 3, cache: str = None) -> dict:
         """Times V-cycles under the result-neutral execution options and keeps

@@ -156,15 +156,35 @@ pgmg_status grid_sweeps(pgmg_handle* h, int l, int mode, int sweeps, unsigned ex
     return PGMG_OK;
 }
 
-// A persistent-sweep wait that ran out (reported once, then cleared).
+// A bounded device wait that ran out -- a grid barrier of the persistent
+// sweeps or an mbarrier wait of the TMA colour pass (reported once, then
+// cleared).
 pgmg_status check_grid(pgmg_handle* h) {
-    if (!h->grid_max) return PGMG_OK;
-    int e = 0;
-    CK(cudaMemcpyAsync(&e, &h->bar->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (!h->grid_max && !h->gs_tma) return PGMG_OK;
+    int e[2] = {0, 0};
+    CK(cudaMemcpyAsync(e, &h->bar->err, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (!e) return PGMG_OK;
+    if (!e[0] && !e[1]) return PGMG_OK;
     CK(cudaMemsetAsync(h->bar, 0, sizeof(GridBar), h->stream));
-    return fail(h, PGMG_ERR_TIMEOUT, "a grid barrier of the persistent sweep kernel ran out of time");
+    if (e[0]) return fail(h, PGMG_ERR_TIMEOUT, "a grid barrier of the persistent sweep kernel ran out of time");
+    return fail(h, PGMG_ERR_TIMEOUT, "an mbarrier wait of the TMA colour pass ran out of time");
+}
+
+// One colour pass of k_gs_colour_tma (128 threads per CTA when the sweep
+// block is 128, else 256).
+template <class T>
+pgmg_status gs_tma_pass(pgmg_handle* h, const LevelGeom& g, View<T>& v, int col, int rev, long nc, unsigned extra) {
+    h->launches++;
+    if (h->gs_block == 128) {
+        CK(launch_k_smem(h->stream, h->pdl, dim3((unsigned)nblk(nc, 128)), dim3(128), gs_tma_smem<T, 128>(),
+                         k_gs_colour_tma<T, 128>, g, v.x, (const T*)v.r, (const T*)v.A, col, rev, &h->bar->tma_err,
+                         extra));
+    } else {
+        CK(launch_k_smem(h->stream, h->pdl, dim3((unsigned)nblk(nc, 256)), dim3(256), gs_tma_smem<T, 256>(),
+                         k_gs_colour_tma<T, 256>, g, v.x, (const T*)v.r, (const T*)v.A, col, rev, &h->bar->tma_err,
+                         extra));
+    }
+    return PGMG_OK;
 }
 
 template <class T>
@@ -234,6 +254,18 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                         LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col, rev);
                     else
                         LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col, rev);
+                }
+        return PGMG_OK;
+    }
+    if (S == 1 && !g.prd && h->gs_tma > 0 && g.npts >= h->gs_tma) {
+        // Stencils and sources staged by bulk copies (k_gs_colour_tma).
+        long nc = (long)g.M2 * g.N2 * g.O2;
+        for (int s = 0; s < sweeps; s++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = colour_seq(pass ? 7 - cc : cc);
+                    int rev = h->gs_alt ? (cc & 1) : 0;
+                    TRY(gs_tma_pass<T>(h, g, v, col, rev, nc, 0u));
                 }
         return PGMG_OK;
     }
@@ -308,10 +340,7 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     Level& F = h->L[l - 1];
     Level& Cl = h->L[l];
     View<T> vf = view<T>(F), vc = view<T>(Cl);
-    if (!F.g.prd && h->fused_restrict) {
-        if (h->fused_restrict == 2) return fused_restrict<T, RrLarge>(h, F, Cl, vf, vc);
-        return fused_restrict<T, RrSmall>(h, F, Cl, vf, vc);
-    }
+    if (!F.g.prd && h->fused_restrict) return fused_restrict<T, RrSmall>(h, F, Cl, vf, vc);
     TRY(residual_level<T>(h, l - 1, vf.res, nullptr));
     if (F.g.prd)
         LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T, true>, F.g, Cl.g, vf.res, vc.r, vc.x);
@@ -718,12 +747,12 @@ pgmg_status prepare_device_kernels(int device) {
     ok = ok && cudaFuncSetAttribute(k_lu_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLuWindowSmemMax) ==
                    cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem) == cudaSuccess;
-    ok = ok && cudaFuncSetAttribute(k_resrestrict<double, RrLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)RrLarge::smem<double>()) == cudaSuccess;
-    ok = ok && cudaFuncSetAttribute(k_resrestrict<float, RrLarge>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)RrLarge::smem<float>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)gs_tma_smem<double, 256>()) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<float, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)gs_tma_smem<float, 256>()) == cudaSuccess;
     cudaFuncAttributes fa;
-    const void* setup_kernels[] = {(const void*)k_lu_build,       (const void*)k_lu_band,
+    const void* setup_kernels[] = {(const void*)k_gs_colour_tma<double, 128>, (const void*)k_gs_colour_tma<float, 128>,(const void*)k_lu_build,       (const void*)k_lu_band,
                                    (const void*)k_lu_inverse,     (const void*)k_rat_bounds,
                                    (const void*)k_rat_fill,       (const void*)k_rat_fill_small,
                                    (const void*)k_assemble_q1,    (const void*)k_rhs_uniform,
@@ -943,11 +972,14 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             h->coarse_shared = value != 0;
             break;
         case PGMG_OPT_FUSED_RESTRICT:
-            if (value < 0 || value > 2) return fail(h, PGMG_ERR_ARG, "fused restriction must be 0, 1 or 2");
-            h->fused_restrict = (int)value;
+            h->fused_restrict = value != 0;
             break;
         case PGMG_OPT_LU_WINDOW:
             h->lu_window = value != 0;
+            break;
+        case PGMG_OPT_GS_TMA:
+            if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_tma must be >= 0");
+            h->gs_tma = value;
             break;
         case PGMG_OPT_GS_PREFETCH:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
@@ -1002,6 +1034,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_COARSE_SHARED: *value = h->coarse_shared; return PGMG_OK;
         case PGMG_OPT_FUSED_RESTRICT: *value = h->fused_restrict; return PGMG_OK;
         case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
+        case PGMG_OPT_GS_TMA: *value = h->gs_tma; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1363,6 +1396,7 @@ struct TuneVal {
     int gs_vec, gs_alt;
     long long gs_prefetch;
     int fused_restrict;
+    long long gs_tma;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1377,7 +1411,8 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->gs_vec = v.gs_vec != 0;
     h->gs_alt = v.gs_alt != 0;
     h->gs_prefetch = v.gs_prefetch;
-    h->fused_restrict = v.fused_restrict;
+    h->fused_restrict = v.fused_restrict != 0;
+    h->gs_tma = v.gs_tma;
     drop_graphs(h);
 }
 
@@ -1441,6 +1476,23 @@ pgmg_status pgmg_dev_profile_vcycle(pgmg_handle* h, int fp32, double* ms, int nm
     return check_grid(h);
 }
 
+pgmg_status pgmg_dev_tma_check(pgmg_handle* h, int level, int run_out) {
+    TRY(check_level(h, level));
+    const LevelGeom& g = h->L[level].g;
+    if (g.prd) return fail(h, PGMG_ERR_UNSUPPORTED, "periodic level");
+    long long keep = h->gs_tma;
+    h->gs_tma = 1;  // makes check_grid read the error word
+    h->x0_zero = false;
+    View<double> v = view<double>(h->L[level]);
+    pgmg_status st = PGMG_OK;
+    // One colour pass (with run_out, every CTA's wait runs out twice: about
+    // a second for the pass).
+    st = gs_tma_pass<double>(h, g, v, colour_seq(0), 0, (long)g.M2 * g.N2 * g.O2, run_out ? 16u : 0u);
+    if (st == PGMG_OK) st = check_grid(h);
+    h->gs_tma = keep;
+    return st;
+}
+
 pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
@@ -1468,7 +1520,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     CK(cudaEventCreate(&e1));
     TuneVal best{h->gs_block,         h->coarse_first,   h->cluster_size, h->pdl ? 1 : 0,
                  h->grid_max,         h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch,
-                 h->fused_restrict, 0};
+                 h->fused_restrict ? 1 : 0, h->gs_tma, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1500,6 +1552,15 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
         TuneVal c = best;
         c.gs_vec = !best.gs_vec;
         st = trial(c);
+    }
+    if (st == PGMG_OK && mc8 && !h->prd) {
+        long long t0 = best.gs_tma;
+        for (long long tm : {0LL, 1LL << 18, 1LL << 22}) {
+            if (st != PGMG_OK || tm == t0) continue;
+            TuneVal c = best;
+            c.gs_tma = tm;
+            st = trial(c);
+        }
     }
     if (st == PGMG_OK && mc8 && !h->prd)
         for (int b : {128, 256, 512}) {
@@ -1544,13 +1605,9 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
         }
     }
     if (st == PGMG_OK && !h->prd) {
-        int f0 = best.fused_restrict;
-        for (int f : {0, 1, 2}) {
-            if (f == f0) continue;
-            TuneVal c = best;
-            c.fused_restrict = f;
-            if ((st = trial(c)) != PGMG_OK) break;
-        }
+        TuneVal c = best;
+        c.fused_restrict = !best.fused_restrict;
+        st = trial(c);
     }
     if (st == PGMG_OK) {
         TuneVal c = best;

@@ -9,6 +9,7 @@
 #include "kernels_core.cuh"
 #include "kernels_grid.cuh"
 #include "kernels_setup.cuh"
+#include "kernels_tma.cuh"
 #include "layout.cuh"
 
 namespace pgmg {
@@ -141,9 +142,13 @@ struct pgmg_handle {
     // (levels whose halo'd x fits in kCoarseXsMax bytes).
     bool coarse_shared = true;
     // Non-periodic restrictions compute their residuals inside the kernel
-    // (k_resrestrict; 1: 32 x 8 coarse tiles over 8 planes, 2: 32 x 16 over
-    // 16) instead of a residual pass plus k_restrict_fast (0).
-    int fused_restrict = 1;
+    // (k_resrestrict) instead of a residual pass plus k_restrict_fast; off by
+    // default (slower, measured), tried by the autotuner.
+    bool fused_restrict = false;
+    // 8-colour levels of at least gs_tma points (one slab, non-periodic)
+    // stage each pass's stencils and sources with bulk copies
+    // (k_gs_colour_tma); 0 = off.
+    long long gs_tma = 0;
     // The coarse LU factorises in a shared-memory band window (k_lu_window)
     // where it fits, instead of the one-block kernel on device memory.
     bool lu_window = true;

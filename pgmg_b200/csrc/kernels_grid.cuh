@@ -26,7 +26,7 @@ struct GridBar {
     unsigned count;  // blocks arrived at the current barrier
     unsigned gen;    // barriers completed
     int err;         // 1: a wait ran out
-    int pad;
+    int tma_err;     // 1: an mbarrier wait of the TMA colour pass (k_gs_colour_tma) ran out
 };
 
 constexpr long kGridSpinLimit = 1L << 21;
