@@ -197,7 +197,7 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           it fits in 220 KiB); 0 = one thread block on the
  *                           dense matrix in device memory.  Same factors bit
  *                           for bit.  Takes effect at the next set-up.
- *   PGMG_OPT_GS_TMA         8-colour levels of at least this many points (one
+ *   PGMG_OPT_GS_TMA         8-colour levels of at most this many points (one
  *                           slab, non-periodic) stage each colour pass's
  *                           stencil coefficients and sources in shared memory
  *                           with bulk copies of the Tensor Memory Accelerator,

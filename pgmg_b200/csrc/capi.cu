@@ -257,7 +257,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 }
         return PGMG_OK;
     }
-    if (S == 1 && !g.prd && h->gs_tma > 0 && g.npts >= h->gs_tma) {
+    if (S == 1 && !g.prd && h->gs_tma > 0 && g.npts <= h->gs_tma) {
         // Stencils and sources staged by bulk copies (k_gs_colour_tma).
         long nc = (long)g.M2 * g.N2 * g.O2;
         for (int s = 0; s < sweeps; s++)
@@ -1481,7 +1481,7 @@ pgmg_status pgmg_dev_tma_check(pgmg_handle* h, int level, int run_out) {
     const LevelGeom& g = h->L[level].g;
     if (g.prd) return fail(h, PGMG_ERR_UNSUPPORTED, "periodic level");
     long long keep = h->gs_tma;
-    h->gs_tma = 1;  // makes check_grid read the error word
+    h->gs_tma = 1LL << 40;  // makes check_grid read the error word
     h->x0_zero = false;
     View<double> v = view<double>(h->L[level]);
     pgmg_status st = PGMG_OK;
@@ -1555,7 +1555,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     }
     if (st == PGMG_OK && mc8 && !h->prd) {
         long long t0 = best.gs_tma;
-        for (long long tm : {0LL, 1LL << 18, 1LL << 22}) {
+        for (long long tm : {0LL, 1LL << 19, 1LL << 22, 1LL << 26}) {
             if (st != PGMG_OK || tm == t0) continue;
             TuneVal c = best;
             c.gs_tma = tm;

@@ -145,7 +145,7 @@ struct pgmg_handle {
     // (k_resrestrict) instead of a residual pass plus k_restrict_fast; off by
     // default (slower, measured), tried by the autotuner.
     bool fused_restrict = false;
-    // 8-colour levels of at least gs_tma points (one slab, non-periodic)
+    // 8-colour levels of at most gs_tma points (one slab, non-periodic)
     // stage each pass's stencils and sources with bulk copies
     // (k_gs_colour_tma); 0 = off.
     long long gs_tma = 0;

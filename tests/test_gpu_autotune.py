@@ -239,7 +239,7 @@ def test_gs_tma_bitwise(mno, precision, block):
     B = make(mno, precision)
     for G in (A, B):
         G.set_option(P.OPT_GS_BLOCK, block)
-    B.set_option(P.OPT_GS_TMA, 1)
+    B.set_option(P.OPT_GS_TMA, 10 ** 9)  # every level the grid kernels sweep
     for _ in range(2):
         A.v_cycle(0)
         B.v_cycle(0)
