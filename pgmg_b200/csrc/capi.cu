@@ -318,7 +318,7 @@ pgmg_status residual_level(pgmg_handle* h, int l, T* out, double* partials) {
     Level& L = h->L[l];
     View<T> v = view<T>(L);
     const LevelGeom& g = L.g;
-    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    dim3 grid((unsigned)(8 * nblk((long)g.M2 * g.N2 * g.O2)));  // colours interleaved
     LAUNCH(grid, kBlock, k_residual<T, T, true>, g, v.x, v.r, v.A, out, partials);
     return PGMG_OK;
 }
@@ -658,7 +658,7 @@ pgmg_status add_correction(pgmg_handle* h) {
 pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double* rhs2) {
     Level& L0 = h->L[0];
     const LevelGeom& g = L0.g;
-    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    dim3 grid((unsigned)(8 * nblk((long)g.M2 * g.N2 * g.O2)));  // colours interleaved
     if (res2 || rhs2) TRY(check_begin(h));
     LAUNCH(grid, kBlock, k_residual<double, float, true>, g, L0.x64, L0.r64, L0.A64, L0.r32,
            (res2 || rhs2) ? h->partials : nullptr);
@@ -692,7 +692,7 @@ pgmg_status lu_setup(pgmg_handle* h) {
         int kb = L.g.prd ? (int)n - 1 : 1 + L.g.m + L.g.m * L.g.n;
         if (kb > (int)n - 1) kb = (int)n - 1;
         size_t wsm = lu_window_smem((int)n, kb, kb);
-        if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax) {
+        if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax && 2 * kb + 1 <= 1024) {
             // The active band window in shared memory (same factors; the
             // limit is set in prepare_device_kernels).
             k_lu_window<<<1, 1024, wsm, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
@@ -1751,7 +1751,7 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
     plan.every = check_every;
     Level& L0 = h->L[0];
     const LevelGeom& g = L0.g;
-    dim3 grid((unsigned)nblk((long)g.M2 * g.N2 * g.O2), 8);
+    dim3 grid((unsigned)(8 * nblk((long)g.M2 * g.N2 * g.O2)));  // colours interleaved
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
     bool mixed = h->dims.precision == PGMG_MIXED;
     plan.rho0 = h->last_rho;

@@ -346,19 +346,31 @@ __device__ __forceinline__ void residual_at(const LevelGeom& g, const T* __restr
 // K5 / residual half of K3: res = r - A x over a whole level (all 27 slots in
 // box order, region.cc:1833-1842), written colour-major to `out` (type TO),
 // with per-block partial sums of res^2 and r^2 (region.cc:1475-1490,
-// 1549-1558) when `partials` is non-null.  Grid: (blocks per colour, 8).
+// 1549-1558) when `partials` is non-null.  1D grid of 8 x (blocks per
+// colour): block q is block q/8 of colour q%8, so the 8 colours of a region
+// run side by side and share its x in L2 (colour by colour, a level whose x
+// exceeds L2 re-reads it from HBM for every colour).  Block (colour c,
+// block k) writes partial pair c * (blocks per colour) + k, the order the
+// reduction sums them in.
+__device__ __forceinline__ void colour_block(unsigned q, unsigned& col, unsigned& blk) {
+    col = q & 7u;
+    blk = q >> 3;
+}
+
 template <class T, class TO, bool EXACT>
 __global__ void __launch_bounds__(kBlock) k_residual(LevelGeom g, const T* __restrict__ x,
                                                      const T* __restrict__ r, const T* __restrict__ A,
                                                      TO* __restrict__ out, double* __restrict__ partials) {
     pdl_enter();
     __shared__ double sh[64];
+    unsigned col, blk;
+    colour_block(blockIdx.x, col, blk);
     double s_res = 0, s_rhs = 0;
-    residual_at<T, TO>(g, x, r, A, out, blockIdx.y, blockIdx.x * (long)blockDim.x + threadIdx.x, s_res, s_rhs);
+    residual_at<T, TO>(g, x, r, A, out, (int)col, blk * (long)blockDim.x + threadIdx.x, s_res, s_rhs);
     if (partials) {
         block_sum2(s_res, s_rhs, sh);
         if (threadIdx.x == 0) {
-            long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
+            long b = (long)col * (gridDim.x >> 3) + blk;
             partials[2 * b] = s_res;
             partials[2 * b + 1] = s_rhs;
         }
@@ -373,9 +385,11 @@ __global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restr
                                                    double* __restrict__ partials) {
     pdl_enter();
     __shared__ double sh[64];
-    int col = blockIdx.y;
+    unsigned ucol, blk;
+    colour_block(blockIdx.x, ucol, blk);
+    const int col = (int)ucol;
     long nc = (long)g.M2 * g.N2 * g.O2;
-    long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long p = blk * (long)blockDim.x + threadIdx.x;
     double s = 0;
     if (p < nc) {
         T rv = r[(long)col * g.Nc + p];
@@ -385,7 +399,7 @@ __global__ void __launch_bounds__(kBlock) k_source(LevelGeom g, const T* __restr
     double s2 = s;
     block_sum2(s, s2, sh);
     if (threadIdx.x == 0) {
-        long b = (long)blockIdx.y * gridDim.x + blockIdx.x;
+        long b = (long)col * (gridDim.x >> 3) + blk;
         partials[2 * b] = s;
         partials[2 * b + 1] = s2;
     }

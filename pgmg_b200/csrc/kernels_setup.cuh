@@ -714,6 +714,15 @@ static __global__ void __launch_bounds__(1024) k_lu_window(double* __restrict__ 
     for (int j = 0; j < n; j++) {
         const int R = min(n - 1, j + kl) - j;
         const int C = min(n - 1, j + kl + ku) - j;
+        // The row and column that enter the window after this step hold
+        // original matrix values (no step has touched them yet): load them
+        // now, so that the load latency overlaps the step.
+        const int nr = j + kl + 1, nc = j + kl + ku + 1;
+        double pre_r = 0.0, pre_c = 0.0;
+        const int cr = j + 1 + tid, ic = j + 1 + tid;  // thread tid: one entry of each
+        const bool has_r = nr < n && cr <= nc && cr < n, has_c = nc < n && ic < nr && ic < n;
+        if (has_r) pre_r = M[nr + (long)cr * n];
+        if (has_c) pre_c = M[ic + (long)nc * n];
         double bv = -1.0;
         int bi = n;
         for (int i = j + tid; i <= j + R; i += blockDim.x) lu_better(fabs(at(i, j)), i, bv, bi);
@@ -778,12 +787,10 @@ static __global__ void __launch_bounds__(1024) k_lu_window(double* __restrict__ 
         for (int i = tid; i <= R; i += blockDim.x) M[(j + i) + (long)j * n] = at(j + i, j);
         for (int k = tid; k < C; k += blockDim.x) M[j + (long)(j + 1 + k) * n] = sU[k];
         __syncthreads();
-        // Slide: row j+kl+1 takes row j's slots, column j+kl+ku+1 column j's.
-        const int nr = j + kl + 1, nc = j + kl + ku + 1;
-        if (nr < n)
-            for (int c = j + 1 + tid; c <= nc && c < n; c += blockDim.x) at(nr, c) = M[nr + (long)c * n];
-        if (nc < n)
-            for (int i = j + 1 + tid; i < nr && i < n; i += blockDim.x) at(i, nc) = M[i + (long)nc * n];
+        // Slide: row j+kl+1 takes row j's slots, column j+kl+ku+1 column j's
+        // (one entry per thread: kl+ku+1 <= blockDim.x, checked by the host).
+        if (has_r) at(nr, cr) = pre_r;
+        if (has_c) at(ic, nc) = pre_c;
         __syncthreads();
     }
 }
