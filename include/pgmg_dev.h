@@ -203,7 +203,13 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           with bulk copies of the Tensor Memory Accelerator,
  *                           the stencils fetched before the pass waits for the
  *                           previous kernel; 0 = off (default).  Same results
- *                           bit for bit.  No counterpart in the reference. */
+ *                           bit for bit.  No counterpart in the reference.
+ *   PGMG_OPT_RAT_TILE       1 = the Galerkin operators of non-periodic coarse
+ *                           levels of more than 20 000 points are built one
+ *                           thread per (coarse point, stencil slot) over
+ *                           shared-memory tiles (default); 0 = one thread per
+ *                           coarse point.  Same operators bit for bit.  Takes
+ *                           effect at the next set-up. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -223,7 +229,8 @@ enum {
     PGMG_OPT_COARSE_SHARED = 16,
     PGMG_OPT_FUSED_RESTRICT = 17,
     PGMG_OPT_LU_WINDOW = 18,
-    PGMG_OPT_GS_TMA = 19
+    PGMG_OPT_GS_TMA = 19,
+    PGMG_OPT_RAT_TILE = 20
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after

@@ -40,6 +40,7 @@ OPT_COARSE_SHARED = 16
 OPT_FUSED_RESTRICT = 17
 OPT_LU_WINDOW = 18
 OPT_GS_TMA = 19
+OPT_RAT_TILE = 20
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",

@@ -981,6 +981,9 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_tma must be >= 0");
             h->gs_tma = value;
             break;
+        case PGMG_OPT_RAT_TILE:
+            h->rat_tile = value != 0;
+            break;
         case PGMG_OPT_GS_PREFETCH:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
             h->gs_prefetch = value;
@@ -1035,6 +1038,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_FUSED_RESTRICT: *value = h->fused_restrict; return PGMG_OK;
         case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
         case PGMG_OPT_GS_TMA: *value = h->gs_tma; return PGMG_OK;
+        case PGMG_OPT_RAT_TILE: *value = h->rat_tile; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1165,7 +1169,7 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
         if (Cl.g.npts <= kRatSmallMax) {
             k_rat_fill_small<<<nblk(Cl.g.npts * 32, kRatSmallBlock), kRatSmallBlock, 0, h->stream>>>(F.g, Cl.g, F.A64,
                                                                                                    F.S, Cl.A64);
-        } else if (!F.g.prd) {
+        } else if (!F.g.prd && h->rat_tile) {
             dim3 grid((unsigned)((Cl.g.m + kRtX - 1) / kRtX), (unsigned)Cl.g.n, (unsigned)((Cl.g.o + kRtKC - 1) / kRtKC));
             k_rat_tile<<<grid, kRtThreads, kRtSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         } else {

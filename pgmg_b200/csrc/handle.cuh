@@ -152,6 +152,9 @@ struct pgmg_handle {
     // The coarse LU factorises in a shared-memory band window (k_lu_window)
     // where it fits, instead of the one-block kernel on device memory.
     bool lu_window = true;
+    // Galerkin operators of large non-periodic levels by k_rat_tile (one
+    // thread per coarse point and slot) instead of k_rat_fill.
+    bool rat_tile = true;
     int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident
