@@ -209,7 +209,13 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           thread per (coarse point, stencil slot) over
  *                           shared-memory tiles (default); 0 = one thread per
  *                           coarse point.  Same operators bit for bit.  Takes
- *                           effect at the next set-up. */
+ *                           effect at the next set-up.
+ *   PGMG_OPT_GS_L2_PREFETCH 8-colour levels of at most this many points (that
+ *                           PGMG_OPT_GS_PREFETCH covers) prefetch the next
+ *                           colour pass's stencils and sources into L2 with
+ *                           bulk prefetches at the start of each pass; 0 =
+ *                           off (default).  Same results.  No counterpart in
+ *                           the reference. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -230,14 +236,16 @@ enum {
     PGMG_OPT_FUSED_RESTRICT = 17,
     PGMG_OPT_LU_WINDOW = 18,
     PGMG_OPT_GS_TMA = 19,
-    PGMG_OPT_RAT_TILE = 20
+    PGMG_OPT_RAT_TILE = 20,
+    PGMG_OPT_GS_L2_PREFETCH = 21
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
  * one untimed) of this handle's problem under candidate values of the
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
  * PGMG_OPT_GS_ALTERNATE, PGMG_OPT_GS_PREFETCH, PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE,
- * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT, PGMG_OPT_GS_TMA --
+ * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT, PGMG_OPT_GS_TMA,
+ * PGMG_OPT_GS_L2_PREFETCH --
  * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,

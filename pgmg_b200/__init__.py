@@ -41,6 +41,7 @@ OPT_FUSED_RESTRICT = 17
 OPT_LU_WINDOW = 18
 OPT_GS_TMA = 19
 OPT_RAT_TILE = 20
+OPT_GS_L2_PREFETCH = 21
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -289,7 +290,8 @@ class Multigrid:
     TUNED_OPTIONS = {"gs_block": OPT_GS_BLOCK, "cluster_size": OPT_CLUSTER_SIZE, "cluster_first": OPT_CLUSTER_FIRST,
                      "pdl": OPT_PDL, "grid_max": OPT_GRID_MAX, "gs_vector": OPT_GS_VECTOR,
                      "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH,
-                     "fused_restrict": OPT_FUSED_RESTRICT, "gs_tma": OPT_GS_TMA}
+                     "fused_restrict": OPT_FUSED_RESTRICT, "gs_tma": OPT_GS_TMA,
+                     "gs_l2_prefetch": OPT_GS_L2_PREFETCH}
 
     def autotune(self, reps: int = 3, cache: str = None) -> dict:
         """Times V-cycles under the result-neutral execution options and keeps

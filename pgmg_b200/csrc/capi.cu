@@ -273,20 +273,24 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         h->grid_blocks[std::is_same<T, float>::value ? 1 : 0] > 0)
         return grid_sweeps<T>(h, l, mode, sweeps);
     if (S == 1 && !g.prd && g.npts <= h->gs_prefetch) {
-        // Stencil loaded before the launch dependency (k_gs_colour_pf).
+        // Stencil loaded before the launch dependency (k_gs_colour_pf); on
+        // levels of at most gs_l2pf points each pass also prefetches the
+        // next pass's stencils into L2.
         long nc = (long)g.M2 * g.N2 * g.O2;
-        for (int s = 0; s < sweeps; s++)
-            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
-                for (int cc = 0; cc < 8; cc++) {
-                    int col = colour_seq(pass ? 7 - cc : cc);
-                    int rev = h->gs_alt ? (cc & 1) : 0;
-                    if (h->gs_block == 128)
-                        LAUNCH(nblk(nc, 128), 128, k_gs_colour_pf<T, 128>, g, v.x, v.r, v.A, col, rev);
-                    else if (h->gs_block == 512)
-                        LAUNCH(nblk(nc, 512), 512, k_gs_colour_pf<T, 512>, g, v.x, v.r, v.A, col, rev);
-                    else
-                        LAUNCH(nblk(nc, 256), 256, k_gs_colour_pf<T, 256>, g, v.x, v.r, v.A, col, rev);
-                }
+        const int per = mode ? 16 : 8, total = sweeps * per;
+        const bool l2pf = g.npts <= h->gs_l2pf;
+        for (int st = 0; st < total; st++) {
+            int cc = st % per;
+            int col = colour_seq(cc < 8 ? cc : 15 - cc);
+            int nx = st + 1 < total && l2pf ? colour_seq((st + 1) % per < 8 ? (st + 1) % per : 15 - (st + 1) % per) : -1;
+            int rev = h->gs_alt ? (cc & 1) : 0;
+            if (h->gs_block == 128)
+                LAUNCH(nblk(nc, 128), 128, k_gs_colour_pf<T, 128>, g, v.x, v.r, v.A, col, rev, nx);
+            else if (h->gs_block == 512)
+                LAUNCH(nblk(nc, 512), 512, k_gs_colour_pf<T, 512>, g, v.x, v.r, v.A, col, rev, nx);
+            else
+                LAUNCH(nblk(nc, 256), 256, k_gs_colour_pf<T, 256>, g, v.x, v.r, v.A, col, rev, nx);
+        }
         return PGMG_OK;
     }
     for (int s = 0; s < sweeps; s++)
@@ -984,6 +988,10 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_RAT_TILE:
             h->rat_tile = value != 0;
             break;
+        case PGMG_OPT_GS_L2_PREFETCH:
+            if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_l2_prefetch must be >= 0");
+            h->gs_l2pf = value;
+            break;
         case PGMG_OPT_GS_PREFETCH:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_prefetch must be >= 0");
             h->gs_prefetch = value;
@@ -1039,6 +1047,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
         case PGMG_OPT_GS_TMA: *value = h->gs_tma; return PGMG_OK;
         case PGMG_OPT_RAT_TILE: *value = h->rat_tile; return PGMG_OK;
+        case PGMG_OPT_GS_L2_PREFETCH: *value = h->gs_l2pf; return PGMG_OK;
     }
     return fail(h, PGMG_ERR_ARG, "unknown option %d", key);
 }
@@ -1401,6 +1410,7 @@ struct TuneVal {
     long long gs_prefetch;
     int fused_restrict;
     long long gs_tma;
+    long long gs_l2pf;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1417,6 +1427,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->gs_prefetch = v.gs_prefetch;
     h->fused_restrict = v.fused_restrict != 0;
     h->gs_tma = v.gs_tma;
+    h->gs_l2pf = v.gs_l2pf;
     drop_graphs(h);
 }
 
@@ -1524,7 +1535,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     CK(cudaEventCreate(&e1));
     TuneVal best{h->gs_block,         h->coarse_first,   h->cluster_size, h->pdl ? 1 : 0,
                  h->grid_max,         h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch,
-                 h->fused_restrict ? 1 : 0, h->gs_tma, 0};
+                 h->fused_restrict ? 1 : 0, h->gs_tma, h->gs_l2pf, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1556,6 +1567,15 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
         TuneVal c = best;
         c.gs_vec = !best.gs_vec;
         st = trial(c);
+    }
+    if (st == PGMG_OK && mc8 && !h->prd) {
+        long long q0 = best.gs_l2pf;
+        for (long long lp : {0LL, 1LL << 19, 1LL << 22}) {
+            if (st != PGMG_OK || lp == q0) continue;
+            TuneVal c = best;
+            c.gs_l2pf = lp;
+            st = trial(c);
+        }
     }
     if (st == PGMG_OK && mc8 && !h->prd) {
         long long t0 = best.gs_tma;

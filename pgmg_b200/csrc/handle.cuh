@@ -155,6 +155,9 @@ struct pgmg_handle {
     // Galerkin operators of large non-periodic levels by k_rat_tile (one
     // thread per coarse point and slot) instead of k_rat_fill.
     bool rat_tile = true;
+    // k_gs_colour_pf levels of at most gs_l2pf points prefetch the next
+    // pass's stencils into L2 (0 = off).
+    long long gs_l2pf = 0;
     int inner_digits = 5;  // mixed precision: at most a 10^-inner_digits reduction per refinement step
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident

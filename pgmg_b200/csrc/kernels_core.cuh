@@ -126,11 +126,35 @@ __global__ void __launch_bounds__(BS) k_gs_colour_v(LevelGeom g, T* x, const T* 
 // written only at set-up -- are loaded first; only then does it wait for
 // the previous kernel and load the source and the neighbours' x, which that
 // kernel may have written.  Same arithmetic as gs_value.
+// Prefetch into L2 (cp.async.bulk.prefetch, the TMA's bulk prefetch) of the
+// stencil runs and the source run of colour `col` for colour points [p0,
+// p0 + L): 16-byte-aligned starts (slot planes on 256-byte boundaries, p0 a
+// multiple of the block size), sizes rounded up to 16 bytes inside the
+// plane's padding.  A cache hint: it changes no result.
+template <class T>
+__device__ __forceinline__ void prefetch_colour_l2(const LevelGeom& g, const T* A, const T* r, int col, long p0,
+                                                   long L) {
+    const unsigned bytes = (unsigned)((L * (long)sizeof(T) + 15) & ~15L);
+    const T* Ap = A + (long)col * 27 * g.Nc + p0;
+#pragma unroll 1
+    for (int q = 0; q < 27; q++)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Ap + q * g.Nc), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(r + (long)col * g.Nc + p0), "r"(bytes) : "memory");
+}
+
+// next >= 0: thread 0 of each block also prefetches colour `next`'s stencil
+// and source for the block's points into L2 at the start, so that on levels
+// whose colour fits in L2 the next pass reads them from there while this one
+// runs.
 template <class T, int BS>
 __global__ void __launch_bounds__(BS) k_gs_colour_pf(LevelGeom g, T* x, const T* __restrict__ r,
-                                                     const T* __restrict__ A, int col, int rev) {
+                                                     const T* __restrict__ A, int col, int rev, int next) {
     long nc = (long)g.M2 * g.N2 * g.O2;
     unsigned b = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    if (next >= 0 && threadIdx.x == 0) {
+        long p0 = b * (long)BS;
+        prefetch_colour_l2<T>(g, A, r, next, p0, nc - p0 < BS ? nc - p0 : BS);
+    }
     long p = b * (long)BS + threadIdx.x;
     bool ok = p < nc;
     int i = 0, j = 0, k = 0;

@@ -262,3 +262,22 @@ def test_tma_bounded_wait():
     A.clear_x(0)
     cyc, rr = A.solve(1e-10, 100, 0)
     assert rr < 1e-10
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_gs_l2_prefetch_bitwise(precision):
+    """Prefetching the next colour pass's stencils into L2 changes no
+    iterate (sweeps in both directions: symmetric mode too)."""
+    mno = (97, 81, 65)
+    A = make(mno, precision)
+    B = make(mno, precision)
+    B.set_option(P.OPT_GS_L2_PREFETCH, 10 ** 9)
+    for mode in (0, 1, 0):
+        A.v_cycle(mode)
+        B.v_cycle(mode)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
+    A.clear_x(0)
+    B.clear_x(0)
+    A.solve(1e-10, 100, 0)
+    B.solve(1e-10, 100, 0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
