@@ -193,10 +193,11 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           pass, then the restriction (default: faster on a
  *                           B200).  Same results bit for bit.
  *   PGMG_OPT_LU_WINDOW      1 = the coarsest level's LU factorisation keeps its
- *                           active band window in shared memory (default, where
- *                           it fits in 220 KiB); 0 = one thread block on the
- *                           dense matrix in device memory.  Same factors bit
- *                           for bit.  Takes effect at the next set-up.
+ *                           active band window in shared memory (where it fits
+ *                           in 220 KiB); 0 = one thread block on the dense
+ *                           matrix in device memory (default: faster on a
+ *                           B200).  Same factors bit for bit.  Takes effect at
+ *                           the next set-up.
  *   PGMG_OPT_GS_TMA         8-colour levels of at most this many points (one
  *                           slab, non-periodic) stage each colour pass's
  *                           stencil coefficients and sources in shared memory
@@ -207,9 +208,10 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *   PGMG_OPT_RAT_TILE       1 = the Galerkin operators of non-periodic coarse
  *                           levels of more than 20 000 points are built one
  *                           thread per (coarse point, stencil slot) over
- *                           shared-memory tiles (default); 0 = one thread per
- *                           coarse point.  Same operators bit for bit.  Takes
- *                           effect at the next set-up.
+ *                           shared-memory tiles; 0 = one thread per coarse
+ *                           point (default: faster on a B200).  Same
+ *                           operators bit for bit.  Takes effect at the next
+ *                           set-up.
  *   PGMG_OPT_GS_L2_PREFETCH 8-colour levels of at most this many points (that
  *                           PGMG_OPT_GS_PREFETCH covers) prefetch the next
  *                           colour pass's stencils and sources into L2 with

@@ -319,13 +319,19 @@ def test_sweep_count_options():
 
 
 @pytest.mark.parametrize("mno", [(65, 65, 65), (81, 40, 66), (66, 58, 49), (97, 33, 70)])
-def test_rat_large_levels_bitwise(mno):
-    """Coarse levels of more than 20,000 points (built by the tiled Galerkin
-    kernel, one thread per coarse point and stencil slot): boxes and
-    stencils bit for bit the oracle's, on odd, even and mixed sizes whose
-    tiles are cut at every edge."""
-    G, prob = make(mno)
-    O = oracle_for(mno, prob, G.lu_enabled)
+@pytest.mark.parametrize("rat_tile", [0, 1])
+def test_rat_large_levels_bitwise(mno, rat_tile):
+    """Coarse levels of more than 20,000 points, built one thread per coarse
+    point (default) or by the tiled kernel (one thread per coarse point and
+    stencil slot): boxes and stencils bit for bit the oracle's, on odd, even
+    and mixed sizes whose tiles are cut at every edge."""
+    m, n, o = mno
+    coef, S, r = q1_problem(m, n, o, sigma=1.0, seed=sum(mno))
+    G = P.Multigrid(m, n, o, coarse=P.COARSE_LU_EXACT)
+    G.set_option(P.OPT_RAT_TILE, rat_tile)
+    G.setup_matrices(coef, S)
+    G.setup_fields(r)
+    O = oracle_for(mno, (coef, S, r), G.lu_enabled)
     assert G.nlevels == O.nlevels
     assert G.dims(1)[0] * G.dims(1)[1] * G.dims(1)[2] > 20000
     for l in range(G.nlevels):
