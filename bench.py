@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--device-setup", action="store_true",
                     help="assemble the stencils and the source on the GPU (same values as the host generators)")
     ap.add_argument("--batch-problems", type=int, default=96, help="problems in the batch96 workload")
+    ap.add_argument("--set-option", action="append", default=[], metavar="NAME=VALUE",
+                    help="an execution option (as named in Multigrid.TUNED_OPTIONS) applied after autotuning, "
+                         "e.g. to profile a kernel variant the tuner did not choose; repeatable")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-seq-seconds", type=float, default=60.0,
@@ -161,6 +164,14 @@ def profiled_traffic(name: str):
     except Exception:
         pass
     return None
+
+
+def apply_set_options(G, a):
+    """--set-option NAME=VALUE pairs onto a handle (after its autotuning)."""
+    import pgmg_b200 as P
+    for kv in a.set_option:
+        name, val = kv.split("=", 1)
+        G.set_option(P.Multigrid.TUNED_OPTIONS[name], int(val))
 
 
 def build_problem(m, sigma, seed):
@@ -329,6 +340,7 @@ def run_ours(a):
     # Result-neutral execution options chosen by the library's autotuner
     # (before any timed region).
     tuning = G.autotune(cache=a.tune_cache)
+    apply_set_options(G, a)
 
     def solve_once(H):
         H.clear_x(0)
@@ -400,6 +412,7 @@ def run_ours(a):
         Gm.set_stream(stream.cuda_stream)
         setup(Gm)
         mixed_tuning = Gm.autotune(cache=a.tune_cache)
+        apply_set_options(Gm, a)
         for _ in range(a.warmup):
             mc, mr = solve_once(Gm)
         torch.cuda.synchronize()
