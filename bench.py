@@ -57,8 +57,9 @@ def parse():
                     help="JSON file of autotuner choices: a shape found there is not re-tuned (so that the same "
                          "command run under a profiler uses the options a plain run chose)")
     ap.add_argument("--workload", default="solve257",
-                    choices=["solve257", "small65", "large513", "batch96", "serve"],
-                    help="solve257 is the benchmark line; the others measure the other configurations")
+                    choices=["solve257", "small65", "large513", "batch96", "serve", "entrypoints"],
+                    help="solve257 is the benchmark line; small65 .. serve measure the other configurations; "
+                         "entrypoints times every drop-in entry point on its own at --size")
     ap.add_argument("--profile-mixed", action="store_true",
                     help="only the mixed-precision solves of the benchmark problem (for profiler launch lists)")
     ap.add_argument("--smoother", default="mc8", choices=["mc8", "lex"],
@@ -910,6 +911,125 @@ def run_serve(a):
     print(json.dumps(out))
 
 
+def run_entrypoints(a):
+    """Every drop-in entry point timed on its own (CUDA events, after one
+    untimed call): on an FP64 problem of --size^3 with the cluster tail off,
+    so that the per-level kernels down to the explicit-inverse coarse solve
+    run; the field, stencil and PCG-helper accessors; the mixed set-up; a
+    periodic 64^3 problem; a batch of four 33^3 problems; the no-alloc norms.
+    Each kernel of the library is launched here at least once (for per-kernel
+    profiles of those the benchmark solve does not launch)."""
+    import torch
+
+    import pgmg_b200 as P
+    m, reps = a.size, max(1, a.steps)
+    N = m ** 3
+    st = torch.cuda.Stream()
+    out = {}
+
+    def t(name, fn, nbytes=None):
+        fn()
+        dt, _ = timed(st, fn, reps)
+        out[name] = {"ms": round(dt * 1e3, 4)}
+        if nbytes:
+            out[name]["alg_GBs"] = round(nbytes / dt / 1e9, 1)
+
+    g = P.problem_gauss(m, m, m, a.seed, 8.0)
+    G = P.Multigrid(m, m, m)
+    G.set_stream(st.cuda_stream)
+    t0 = time.perf_counter()
+    G.assemble_q1(g, from_log=True, sigma=a.sigma)
+    G.sync()
+    out["assemble_q1+build_rat (host clock, first call)"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2)}
+    G.rhs_uniform(a.seed)
+    G.set_option(P.OPT_CLUSTER_SIZE, 0)
+    dev = torch.randn(N, dtype=torch.float64, device="cuda")
+    dev2 = torch.empty_like(dev)
+    h = G.handle
+    L = P.lib()
+    t("set_field x (natural -> halo'd)", lambda: G.set_field(0, P.FIELD_X, dev.data_ptr()), 16 * N)
+    t("get_field x", lambda: G.get_field(0, P.FIELD_X, dev2.data_ptr()), 16 * N)
+    t("set_field r (natural -> colour-major)", lambda: G.set_field(0, P.FIELD_R, dev.data_ptr()), 16 * N)
+    t("get_field r", lambda: G.get_field(0, P.FIELD_R, dev2.data_ptr()), 16 * N)
+    t("apply (A x, device pointers)", lambda: L.pgmg_dev_apply(h, 0, dev.data_ptr(), dev2.data_ptr()), 240 * N)
+    t("clear_x", lambda: G.clear_x(0), 8 * N)
+    t("setup_test", lambda: G.setup_test(1, True, 0), 16 * N)
+    t("copy_rhs_to_soln", lambda: G.copy_rhs_to_soln(0), 16 * N)
+    t("l0_error", lambda: G.l0_error(0), 232 * N)
+    t("source_soln_dot", lambda: G.source_soln_dot(0), 16 * N)
+    t("norms", lambda: G.norms(0), 232 * N)
+    t("gauss_seidel mc8 level 0 (one sweep)", lambda: G.gauss_seidel(0, 0, P.SMOOTH_MC8), 240 * N)
+    t("gauss_seidel lex level 0 (one sweep)", lambda: G.gauss_seidel(0, 0, P.SMOOTH_LEX))
+    t("restriction 0 -> 1", lambda: G.restriction(1))
+    t("interpolation 1 -> 0", lambda: G.interpolation(1))
+    t("solve_exact (explicit inverse)", lambda: G.solve_exact())
+    t("v_cycle mc8, per-level kernels", lambda: G.v_cycle(0, P.SMOOTH_MC8))
+    t("fmg_cycle mc8", lambda: G.fmg_cycle(P.SMOOTH_MC8))
+    G.close()
+    del g
+
+    # Stencils uploaded from and read back to the host (natural 27-slot rows).
+    ms = min(m, 65)
+    coef, S = P.problem_q1(ms, ms, ms)
+    H = P.Multigrid(ms, ms, ms)
+    H.set_stream(st.cuda_stream)
+    t(f"setup_matrices {ms}^3 (upload + build_rat)", lambda: H.setup_matrices(coef, S))
+    t(f"get_coef level 0 {ms}^3", lambda: H.get_coef(0))
+    H.close()
+
+    # Mixed precision: FP32 copies of the stencils at set-up.
+    gm = P.problem_gauss(m, m, m, a.seed, 8.0)
+    Hm = P.Multigrid(m, m, m, precision=P.MIXED)
+    Hm.set_stream(st.cuda_stream)
+    t("assemble_q1+build_rat, mixed", lambda: Hm.assemble_q1(gm, from_log=True, sigma=a.sigma))
+    Hm.close()
+    del gm
+
+    # Periodic 64^3: halo images and the periodic transfers.
+    mp = 64
+    Np = mp ** 3
+    base = np.zeros(27)
+    for s in range(27):
+        nd = abs(s % 3 - 1) + abs((s // 3) % 3 - 1) + abs(s // 9 - 1)
+        base[s] = (8.0 / 3.0 + 0.3, 0.0, -1.0 / 6.0, -1.0 / 12.0)[nd]
+    Sp = np.tile(np.array([-1, 2, -1, 2, -1, 2], np.int32), (Np, 1))
+    rp = np.random.default_rng(a.seed).uniform(-1, 1, Np)
+    Hp = P.Multigrid(mp, mp, mp, prd=(True, True, True))
+    Hp.set_stream(st.cuda_stream)
+    Hp.setup_matrices(np.tile(base, (Np, 1)), Sp)
+    Hp.setup_fields(rp)
+    t("v_cycle periodic 64^3", lambda: Hp.v_cycle(0))
+    Hp.close()
+
+    # A batch of four 33^3 problems, mixed precision.
+    hs = []
+    for p in range(4):
+        Gb = P.Multigrid(33, 33, 33, precision=P.MIXED)
+        Gb.assemble_q1(P.problem_gauss(33, 33, 33, a.seed + p, 8.0), from_log=True, sigma=1.0)
+        Gb.rhs_uniform(p)
+        hs.append(Gb)
+    B = P.Batch(4, P.MIXED)
+    for p, Gb in enumerate(hs):
+        B.attach(p, Gb)
+    t("batch of 4 x 33^3, mixed, to 1e-10", lambda: B.solve(a.tol, 100))
+    B.close()
+    for Gb in hs:
+        Gb.close()
+
+    # No-alloc norms on caller-owned arrays (65^3).
+    mn = 65
+    cn, _ = P.problem_q1(mn, mn, mn)
+    dc = torch.from_numpy(np.ascontiguousarray(cn)).cuda()
+    dx = torch.randn(mn ** 3, dtype=torch.float64, device="cuda")
+    dr = torch.randn(mn ** 3, dtype=torch.float64, device="cuda")
+    o2 = torch.zeros(2, dtype=torch.float64, device="cuda")
+    t(f"residual_norms_noalloc {mn}^3",
+      lambda: P.residual_norms_noalloc(mn, mn, mn, dc.data_ptr(), dx.data_ptr(), dr.data_ptr(), o2.data_ptr(),
+                                       st.cuda_stream), 232 * mn ** 3)
+    print(json.dumps({"workload": f"drop-in entry points one by one, {m}^3 FP64 (others as named)",
+                      "unit": "ms per call", "reps": reps, "entry_points": out}))
+
+
 def run_profile_mixed(a):
     import torch
 
@@ -944,6 +1064,8 @@ def main():
         run_batch96(a)
     elif a.workload == "serve":
         run_serve(a)
+    elif a.workload == "entrypoints":
+        run_entrypoints(a)
     elif a.profile_mixed:
         run_profile_mixed(a)
     else:
