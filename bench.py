@@ -447,7 +447,8 @@ def run_ours(a):
                        "levels": G.nlevels, "cycles": cyc_list[-1], "final_relres": final_relres,
                        "smoother": ("lexicographic (wavefront) Gauss-Seidel" if a.smoother == "lex"
                                     else "8-colour Gauss-Seidel"), "coarse": "FP64 LU (explicit inverse)",
-                       "l2": "inputs larger than L2 (3.7 GB stencils)", "setup_s": setup_s,
+                       "l2": f"inputs larger than L2 ({216 * m ** 3 / 1e9:.2f} GB of level-0 stencils)",
+                       "setup_s": setup_s,
                        "host_generation_s": gen_s, "parallelism": f"replicas x{world}", "tuning": tuning,
                        "per_rank_s_per_solve": ms / 1e3},
             "e2e": {"value": rep.per_solve(e2e_ms) / 1e3, "unit": UNIT, "h2d_bytes_per_step": npts * 8,
