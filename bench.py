@@ -75,7 +75,9 @@ def parse():
     ap.add_argument("--serve-seq-seconds", type=float, default=60.0,
                     help="time budget of the one-request-at-a-time comparison")
     ap.add_argument("--serve-sustained-seconds", type=float, default=30.0,
-                    help="length of the second serving run, at 80%% of the saturated throughput (0 = skip)")
+                    help="length of the second serving run, at a fraction of the saturated throughput (0 = skip)")
+    ap.add_argument("--serve-sustained-fraction", type=float, default=0.7,
+                    help="arrival rate of the second serving run as a fraction of the saturated throughput")
     return ap.parse_args()
 
 
@@ -843,11 +845,12 @@ def run_serve(a):
     srv.close()
     del srv
     torch.cuda.empty_cache()
-    # Latency at a load the server sustains: a second open-loop stream at 80 %
-    # of the saturated throughput just measured.  Sustained means the late
-    # requests wait no longer than the early ones (the queue does not grow).
+    # Latency at a load the server sustains: a second open-loop stream at a
+    # fraction (default 70 %) of the saturated throughput just measured.
+    # Sustained means the late requests wait no longer than the early ones
+    # (the queue does not grow).
     if a.serve_sustained_seconds > 0:
-        rate2 = 0.8 * out["value"]
+        rate2 = a.serve_sustained_fraction * out["value"]
         reqs2 = poisson_requests(rate2, a.serve_sustained_seconds, seed=a.seed + 1, reuse=0.2, sizes=(65, 129, 257),
                                  sigma=(0.5, 2.3))
         for r in reqs2:
@@ -1013,6 +1016,13 @@ def run_entrypoints(a):
     for p, Gb in enumerate(hs):
         B.attach(p, Gb)
     t("batch of 4 x 33^3, mixed, to 1e-10", lambda: B.solve(a.tol, 100))
+
+    def stepwise():
+        for p in range(4):
+            B.begin(p)
+        while B.step(a.tol, 100) > 0:
+            pass
+    t("the same batch by begin + step (continuous batching)", stepwise)
     B.close()
     for Gb in hs:
         Gb.close()
