@@ -55,8 +55,8 @@ typedef enum {
     PGMG_ERR_CUDA = 8,         /* a CUDA runtime call failed                */
     PGMG_ERR_TIMEOUT = 9,      /* a bounded device wait ran out             */
     PGMG_ERR_ADMISSION = 10,   /* request does not fit the memory cap       */
-    PGMG_ERR_UNSUPPORTED = 11, /* configuration not supported (e.g. a periodic
-                                  axis odd on a level above the coarsest) */
+    PGMG_ERR_UNSUPPORTED = 11, /* configuration not supported (e.g. the Q1
+                                  generator on a periodic grid)            */
     PGMG_ERR_NO_DEVICE = 12    /* no CUDA device visible                    */
 } pgmg_status;
 
@@ -97,9 +97,8 @@ typedef struct pgmg_handle pgmg_handle;
  * (geometry.cc:12-26) on one process, plus the run-time choices. */
 typedef struct {
     int m, n, o;              /* global grid size                          */
-    int x_prd, y_prd, z_prd;  /* periodicity (non-zero: periodic; the axis
-                                 must be even on every level but the
-                                 coarsest; coarse size (m+1)>>1, region.cc:14) */
+    int x_prd, y_prd, z_prd;  /* periodicity (non-zero: periodic; any size,
+                                 coarse size (m+1)>>1, region.cc:14)      */
     int precision;            /* PGMG_FP64 or PGMG_MIXED                    */
     int coarse;               /* PGMG_COARSE_LU or PGMG_COARSE_GS           */
     int smoother;             /* default smoother of pgmg_dev_vcycle        */
@@ -174,8 +173,10 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           those paths.  No counterpart in the reference.
  *   PGMG_OPT_INNER_DIGITS   mixed precision, adaptive schedule: the FP32
  *                           V-cycles of one refinement step are asked for at
- *                           most a 10^-d predicted reduction (1..7, default 5).
- *                           Changes the iterates (not the tolerance reached).
+ *                           most a 10^-d predicted reduction (1..7, default 5;
+ *                           d+1 while the solve gains more than a digit per
+ *                           cycle).  Changes the iterates (not the tolerance
+ *                           reached).
  *   PGMG_OPT_GS_BLOCK       threads per block of the 8-colour sweep kernel:
  *                           128, 256 (default) or 512.  No counterpart in the
  *                           reference.

@@ -193,11 +193,7 @@ __device__ inline int bplan_next(const BPlan& P, int every, int mixed, int nc, d
         if (n < 1) n = 1;
         if (n > 1 && P.last_r * pow(q, n - 1) < kSlack * tol) n--;
         nx = nc + n;
-        if (mixed) {
-            int cap = (int)floor(log(kInnerReduction) / log(q));
-            cap = cap < 1 ? 1 : cap > kInnerMax ? kInnerMax : cap;
-            if (nx > nc + cap) nx = nc + cap;
-        }
+        if (mixed) nx = nc + ir_inner_cycles(n, q, kInnerDigits);
     }
     if (nx > max_cycles) nx = max_cycles;
     if (nx < nc + 1) nx = nc + 1;

@@ -751,6 +751,7 @@ pgmg_status prepare_device_kernels(int device) {
     ok = ok && cudaFuncSetAttribute(k_lu_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLuWindowSmemMax) ==
                    cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_rat_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRatSmem) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)gs_tma_smem<double, 256>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<float, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1182,7 +1183,7 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
             dim3 grid((unsigned)((Cl.g.m + kRtX - 1) / kRtX), (unsigned)Cl.g.n, (unsigned)((Cl.g.o + kRtKC - 1) / kRtKC));
             k_rat_tile<<<grid, kRtThreads, kRtSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         } else {
-            k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, 0, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+            k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, kRatSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         }
         CKL();
     }
@@ -1838,15 +1839,11 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
         if (mixed) {
             // One refinement step: A32 e = r32 solved by `inner` FP32
             // V-cycles from e = 0, then x64 += e.  The count is the number of
-            // cycles the check schedule expects to run before its next check,
-            // capped so that one step asks the FP32 iteration for no more than
-            // a 1e-5 reduction (beyond that FP32 rounding, not the cycle count,
-            // limits what the correction can gain).
+            // cycles the check schedule expects to run before its next check;
+            // with the adaptive schedule it is limited by ir_inner_cycles to
+            // what one FP32 solve can usefully reduce.
             int inner = next_check - nc;
-            double q = plan.rho();
-            int cap = q > 0 && q < 0.9 ? (int)floor(-h->inner_digits * log(10.0) / log(q)) : 1;
-            cap = cap < 1 ? 1 : cap > kInnerMax ? kInnerMax : cap;
-            if (plan.every == 0 && inner > cap) inner = cap;
+            if (plan.every == 0) inner = ir_inner_cycles(inner, plan.rho(), h->inner_digits);
             if (inner > max_cycles - nc) inner = max_cycles - nc;
             if (inner < 1) inner = 1;
             if (!spec) {

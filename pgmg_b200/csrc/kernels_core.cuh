@@ -595,13 +595,6 @@ __global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom 
     interp_cube_at<T>(gf, gc, xf, xcv, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
-// One axis of a coarse point whose transfer is the interior one: both cubes
-// I-1 and I exist, have their upper point and are not snapped, so the fine
-// points 2I-1, 2I, 2I+1 transfer with weights 1/2, 1, 1/2.
-__device__ __forceinline__ bool inner_axis(int I, int ma) {
-    return I >= 1 && I <= cube_last(ma) && has_upper(I, ma) && !snapped(I, ma);
-}
-
 // Restriction of a non-periodic level.  Coarse points interior on all three
 // axes run restrict_sum's loops with the weights known at compile time (the
 // same contributions in the same order, all 27 loads issued first); the

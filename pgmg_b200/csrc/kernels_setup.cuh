@@ -72,23 +72,16 @@ static __global__ void __launch_bounds__(256) k_rat_bounds(LevelGeom gf, LevelGe
 // axis, and A_add (:1173-1180) adds it to this coarse point's row.  Products
 // by powers of two are exact, sums are rounded one by one (no fused
 // multiply-add), so the result matches the reference bit for bit.
-// Grid: one thread per coarse point.  Each fine point's 27 coefficients are
-// loaded at once into the thread's column of a shared-memory tile (27
-// independent loads, one memory latency) and its ~90 terms read them there.
-// Output: colour-major coarse stencils.
-constexpr int kRatBlock = 128;
+// One thread per coarse point.  Output: colour-major coarse stencils.
+constexpr int kRatBlock = 256;
 
-static __global__ void __launch_bounds__(kRatBlock, 4) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
-                                                        const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
-    __shared__ double sa[27 * kRatBlock];
-    double* my = sa + threadIdx.x;
-    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (q >= gc.npts) return;
-    int I, J, K;
-    decode_nat(gc, q, I, J, K);
-    double acc[27];
-#pragma unroll
-    for (int s = 0; s < 27; s++) acc[s] = 0.0;
+// The general gather, for any coarse point (boundaries, snapped cubes,
+// periodic images, cropped boxes).  Each fine point's 27 coefficients are
+// loaded at once into the thread's column `my` of a shared-memory tile (27
+// independent loads, one memory latency) and its terms read them there.
+static __device__ __noinline__ void rat_general(const LevelGeom& gf, const double* __restrict__ Af,
+                                         const int8_t* __restrict__ Sf, int I, int J, int K, double* my,
+                                         double* acc) {
     const bool qx = px(gf), qy = py(gf), qz = pz(gf);
     int lx = cube_last(gf.m, qx), ly = cube_last(gf.n, qy), lz = cube_last(gf.o, qz);
     for (int cz = K - 1; cz <= K; cz++) {
@@ -153,10 +146,152 @@ static __global__ void __launch_bounds__(kRatBlock, 4) k_rat_fill(LevelGeom gf, 
             }
         }
     }
-    int col = gc.colour(I, J, K);
-    long c = gc.cidx(I, J, K);
+}
+
+// The interior gather.  A coarse point of a non-periodic level that is
+// interior on every axis (inner_axis: fine points 2I-1, 2I, 2I+1 transfer
+// with weights 1/2, 1, 1/2) and whose 27 fine points all have the full box
+// [-1,2)^3 takes rat_general's path with every bound, weight and slot known
+// at compile time: per axis a fine point at offset o from 2I reaches coarse
+// offsets v in [-1,1) (o = -1), [-1,2) (o = 0) or [0,2) (o = 1), gathering
+// fine offsets [2v-1, 2v+2) cropped to its box [o-1, o+2); igrid_map's
+// coincident point is 2v.  The fine points are visited in the same scan order,
+// each At sums its terms in the same (kk, jj, ii) order and each accumulator
+// receives the same additions in the same order, so the result is rat_general's
+// bit for bit.  With no data-dependent control flow the fine point's 27
+// coefficients stay in registers and its At sums are independent chains the
+// scheduler can interleave; the 27 accumulators live in the thread's column
+// of the shared-memory tile (in registers, beside the coefficients and the
+// chains in flight, they spill).
+struct RatScan {
+    int o[27][3];
+};
+__host__ __device__ constexpr RatScan rat_scan() {
+    RatScan r{};
+    int n = 0;
+    for (int az = 0; az < 2; az++)
+        for (int ay = 0; ay < 2; ay++)
+            for (int ax = 0; ax < 2; ax++)
+                for (int dz = 0; dz < 2; dz++)
+                    for (int dy = 0; dy < 2; dy++)
+                        for (int dx = 0; dx < 2; dx++) {
+                            const int oz = 2 * az + dz - 2, oy = 2 * ay + dy - 2, ox = 2 * ax + dx - 2;
+                            if (ox < -1 || oy < -1 || oz < -1) continue;
+                            r.o[n][0] = ox;
+                            r.o[n][1] = oy;
+                            r.o[n][2] = oz;
+                            n++;
+                        }
+    return r;
+}
+__host__ __device__ constexpr int rat_imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int rat_imin(int a, int b) { return a < b ? a : b; }
+
+template <int OX, int OY, int OZ>
+__device__ __forceinline__ void rat_fast_fine(const double* __restrict__ fa, long nc, double* acc) {
+    double h[27];
 #pragma unroll
-    for (int s = 0; s < 27; s++) Ac[((long)col * 27 + s) * gc.Nc + c] = acc[s];
+    for (int u = 0; u < 27; u++) h[u] = __dmul_rn(0.125, __ldg(fa + u * nc));
+    constexpr double fac = (OX ? 0.5 : 1.0) * (OY ? 0.5 : 1.0) * (OZ ? 0.5 : 1.0);
+#pragma unroll
+    for (int vz = (OZ == 1 ? 0 : -1); vz < (OZ == -1 ? 1 : 2); vz++)
+#pragma unroll
+        for (int vy = (OY == 1 ? 0 : -1); vy < (OY == -1 ? 1 : 2); vy++)
+#pragma unroll
+            for (int vx = (OX == 1 ? 0 : -1); vx < (OX == -1 ? 1 : 2); vx++) {
+                double At = 0.0;
+#pragma unroll
+                for (int kk = rat_imax(2 * vz - 1, OZ - 1); kk < rat_imin(2 * vz + 2, OZ + 2); kk++) {
+                    const double kfac = kk == 2 * vz ? 1.0 : 0.5;
+#pragma unroll
+                    for (int jj = rat_imax(2 * vy - 1, OY - 1); jj < rat_imin(2 * vy + 2, OY + 2); jj++) {
+                        const double jkfac = jj == 2 * vy ? kfac : 0.5 * kfac;
+#pragma unroll
+                        for (int ii = rat_imax(2 * vx - 1, OX - 1); ii < rat_imin(2 * vx + 2, OX + 2); ii++) {
+                            const int slot = (ii - OX + 1) + 3 * (jj - OY + 1) + 9 * (kk - OZ + 1);
+                            At = __dadd_rn(At, __dmul_rn(h[slot], ii == 2 * vx ? jkfac : 0.5 * jkfac));
+                        }
+                    }
+                }
+                const int s = (vx + 1) + 3 * (vy + 1) + 9 * (vz + 1);
+                acc[s * kRatBlock] = __dadd_rn(acc[s * kRatBlock], __dmul_rn(At, fac));
+            }
+}
+
+// Fine point n (0..26, scan order) of the interior gather.  Called from a
+// loop that is not unrolled, so the compiler does not hoist the loads of
+// later fine points into this one's registers.
+template <int N>
+__device__ __forceinline__ void rat_fast_step(int n, const LevelGeom& gf, const double* __restrict__ Af, int I,
+                                              int J, int K, double* acc) {
+    constexpr RatScan R = rat_scan();
+    constexpr int OX = R.o[N][0], OY = R.o[N][1], OZ = R.o[N][2];
+    if (n == N) {
+        const int ti = 2 * I + OX, tj = 2 * J + OY, tk = 2 * K + OZ;
+        rat_fast_fine<OX, OY, OZ>(Af + (long)gf.colour(ti, tj, tk) * 27 * gf.Nc + gf.cidx(ti, tj, tk), gf.Nc,
+                                  acc);
+        return;
+    }
+    if constexpr (N + 1 < 27) rat_fast_step<N + 1>(n, gf, Af, I, J, K, acc);
+}
+
+// Whether coarse point (I,J,K) takes the interior gather: non-periodic
+// level, interior on every axis, all 27 fine boxes [-1,2)^3 (each box is six
+// int8 at an even offset, read as three 16-bit words (lo, hi) = (-1, 2)).
+__device__ __forceinline__ bool rat_interior(const LevelGeom& gf, const int8_t* __restrict__ Sf, int I, int J,
+                                             int K) {
+    if (gf.prd || !(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o))) return false;
+    bool full = true;
+#pragma unroll
+    for (int oz = -1; oz <= 1; oz++)
+#pragma unroll
+        for (int oy = -1; oy <= 1; oy++)
+#pragma unroll
+            for (int ox = -1; ox <= 1; ox++) {
+                const uint16_t* b =
+                    reinterpret_cast<const uint16_t*>(Sf + 6 * gf.pi(2 * I + ox, 2 * J + oy, 2 * K + oz));
+                full = full && __ldg(b) == 0x02FFu && __ldg(b + 1) == 0x02FFu && __ldg(b + 2) == 0x02FFu;
+            }
+    return full;
+}
+
+// The block's interior points walk the 27 fine points in lock step
+// (a barrier after each), so that the warps of an SM run one fine point's
+// code at a time: unrolled, the 27 fine points are ~100 KB of instructions,
+// which warps at different fine points would keep evicting from the
+// instruction cache.  The block's other points take rat_general afterwards.
+// Dynamic shared memory: kRatSmem (the accumulators or the coefficient
+// columns, one column of 27 per thread).
+constexpr size_t kRatSmem = 27 * kRatBlock * sizeof(double);
+
+static __global__ void __launch_bounds__(kRatBlock, 2) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
+                                                        const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
+    extern __shared__ double sa[];
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const bool valid = q < gc.npts;
+    int I = 0, J = 0, K = 0;
+    if (valid) decode_nat(gc, q, I, J, K);
+    const bool fast = valid && rat_interior(gf, Sf, I, J, K);
+    double* col = sa + threadIdx.x;  // this thread's column: element s at col[s * kRatBlock]
+    double* out = nullptr;
+    if (valid) out = Ac + (long)gc.colour(I, J, K) * 27 * gc.Nc + gc.cidx(I, J, K);
+    if (__syncthreads_or(fast)) {
+        if (fast)
+            for (int s = 0; s < 27; s++) col[s * kRatBlock] = 0.0;
+#pragma unroll 1
+        for (int n = 0; n < 27; n++) {
+            if (fast) rat_fast_step<0>(n, gf, Af, I, J, K, col);
+            __syncthreads();
+        }
+        if (fast)
+            for (int s = 0; s < 27; s++) out[(long)s * gc.Nc] = col[s * kRatBlock];
+    }
+    if (valid && !fast) {
+        double acc[27];
+        for (int s = 0; s < 27; s++) acc[s] = 0.0;
+        rat_general(gf, Af, Sf, I, J, K, col, acc);
+        for (int s = 0; s < 27; s++) out[(long)s * gc.Nc] = acc[s];
+    }
 }
 
 // k_rat_fill for small coarse levels, where one thread per coarse point

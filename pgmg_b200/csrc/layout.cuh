@@ -140,6 +140,12 @@ __host__ __device__ inline int cube_last(int ma, bool p = false) {
 }
 __host__ __device__ inline bool has_upper(int C, int ma, bool p = false) { return even_prd(ma, p) || 2 * C + 1 < ma; }
 __host__ __device__ inline bool snapped(int C, int ma, bool p = false) { return !p && !(ma & 1) && C == cube_last(ma); }
+// One axis of a coarse point whose transfer is the interior one: both cubes
+// I-1 and I exist, have their upper point and are not snapped, so the fine
+// points 2I-1, 2I, 2I+1 transfer with weights 1/2, 1, 1/2.
+__host__ __device__ inline bool inner_axis(int I, int ma) {
+    return I >= 1 && I <= cube_last(ma) && has_upper(I, ma) && !snapped(I, ma);
+}
 __host__ __device__ inline int wrap(int v, int size, bool p) {
     return p ? (v < 0 ? v + size : (v >= size ? v - size : v)) : v;
 }

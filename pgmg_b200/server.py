@@ -107,6 +107,7 @@ class FieldPool:
         self.width = width
         self.fields = {}
         self.lock = threading.Lock()
+        self.stream = None
 
     def get(self, shape, fid: int):
         key = (tuple(shape), fid)
@@ -115,8 +116,15 @@ class FieldPool:
                 import torch
                 m, n, o = shape
                 g = problem_gauss(m, n, o, 1000 + 7919 * fid + 31 * m + 17 * n + o, self.width)
-                t = torch.from_numpy(g).to(f"cuda:{self.device}")
-                torch.cuda.synchronize(self.device)
+                # Uploaded on a stream of its own and waited for on that
+                # stream only: a device-wide synchronisation from this thread
+                # would break a CUDA-graph capture the serving loop may have
+                # in progress on another stream.
+                if self.stream is None:
+                    self.stream = torch.cuda.Stream(self.device)
+                with torch.cuda.stream(self.stream):
+                    t = torch.from_numpy(g).to(f"cuda:{self.device}")
+                self.stream.synchronize()
                 self.fields[key] = t
             return self.fields[key]
 
