@@ -193,12 +193,12 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           residual array in device memory); 0 = a residual
  *                           pass, then the restriction (default: faster on a
  *                           B200).  Same results bit for bit.
- *   PGMG_OPT_LU_WINDOW      1 = the coarsest level's LU factorisation keeps its
- *                           active band window in shared memory (where it fits
- *                           in 220 KiB); 0 = one thread block on the dense
- *                           matrix in device memory (default: faster on a
- *                           B200).  Same factors bit for bit.  Takes effect at
- *                           the next set-up.
+ *   PGMG_OPT_LU_WINDOW      1 (default) = the coarsest level's LU
+ *                           factorisation keeps its active band window in
+ *                           shared memory (where it fits in 220 KiB and the
+ *                           bandwidth is at most 128); 0 = one thread block on
+ *                           the dense matrix in device memory.  Same factors
+ *                           bit for bit.  Takes effect at the next set-up.
  *   PGMG_OPT_GS_TMA         8-colour levels of at most this many points (one
  *                           slab, non-periodic) stage each colour pass's
  *                           stencil coefficients and sources in shared memory

@@ -696,9 +696,10 @@ pgmg_status lu_setup(pgmg_handle* h) {
         int kb = L.g.prd ? (int)n - 1 : 1 + L.g.m + L.g.m * L.g.n;
         if (kb > (int)n - 1) kb = (int)n - 1;
         size_t wsm = lu_window_smem((int)n, kb, kb);
-        if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax && 2 * kb + 1 <= 1024) {
+        if (h->lu_window && !L.g.prd && wsm <= kLuWindowSmemMax && kb <= 128) {
             // The active band window in shared memory (same factors; the
-            // limit is set in prepare_device_kernels).
+            // limit is set in prepare_device_kernels; a lane updates at most
+            // 4 rows, so kl <= 128).
             k_lu_window<<<1, 1024, wsm, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);
         } else {
             k_lu_band<<<1, 1024, 0, h->stream>>>(h->M, (int)n, kb, kb, h->piv, h->info);

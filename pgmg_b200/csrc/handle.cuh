@@ -169,9 +169,8 @@ struct pgmg_handle {
     // (k_gs_colour_tma); 0 = off.
     long long gs_tma = 0;
     // The coarse LU factorises in a shared-memory band window (k_lu_window)
-    // where it fits, instead of the one-block kernel on device memory (off:
-    // measured slower).
-    bool lu_window = false;
+    // where it fits, instead of the one-block kernel on device memory.
+    bool lu_window = true;
     // Galerkin operators of large non-periodic levels by k_rat_tile (one
     // thread per coarse point and slot) instead of k_rat_fill (off: measured
     // slower).

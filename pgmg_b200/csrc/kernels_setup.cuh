@@ -722,12 +722,7 @@ static __global__ void __launch_bounds__(256) k_rhs_uniform(LevelGeom g, uint64_
 }
 
 // ---------------------------------------------------------------------------
-// The whole LU factorisation of the coarsest level in one thread-block
-// cluster: per column, pivot search (each CTA's candidate to global scratch,
-// then every thread picks the first largest), row swap, scaling and the
-// rank-1 update, separated by hardware cluster barriers.  Every matrix entry
-// sees exactly the operations of k_lu_pivot / k_lu_update, so the factors are
-// bit for bit those of the per-column launches.  scratch: 2*CTAs doubles.
+// Pivot candidate order of the LU kernels: larger |value|, then the first row.
 __device__ __forceinline__ void lu_better(double v, int i, double& bv, int& bi) {
     if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
 }
@@ -811,123 +806,208 @@ static __global__ void __launch_bounds__(1024) k_lu_band(double* __restrict__ M,
 // The same factorisation with the active window in shared memory.  At step
 // j only rows j..j+kl and columns j..j+kl+ku can change (above), so the
 // kernel keeps that window -- (kl+1) x (kl+ku+1) doubles, rows and columns
-// stored circularly by index modulo the window size -- and streams the
-// matrix through it: a row or column enters from the dense matrix the step
-// before it is first needed (no earlier step has touched it) and leaves when
-// its last entry is final (column j and row j after step j).  The row
-// interchange of step j also swaps the two rows' multipliers left of
-// column j, which lie in the dense matrix: row_first[i] tracks the first
-// column at which the row now at position i holds a multiplier (rows carry
-// it when they are interchanged), so the swap covers exactly the columns
-// where either row can be non-zero.  Every entry receives the operations of
-// k_lu_band in the same order, so the factors and pivots are identical.
+// stored circularly (row i in slot i mod (kl+1), column c in slot
+// c mod (kl+ku+1), the slots of a step's rows and columns found by counting
+// from the step's first slot, never by a division) -- and streams the matrix
+// through it: a row or column enters from the dense matrix in the step before
+// it is first needed (no earlier step has touched it; its loads are issued at
+// the start of that step) and leaves when its entries are final (column j and
+// row j, written to the dense matrix in step j).  Per step: the swap, scaling
+// and leaving writes; a barrier; the rank-1 update (warp w: columns 1+w,
+// 33+w, ...; lanes: rows), the entering row and column, and warp 0's pivot
+// search of the next column, which warp 0 has just updated itself; a
+// barrier.  The row interchanges' effect on the multipliers already written
+// (left of the step's column) is applied at the end, column by column in
+// step order, which leaves the same dense factors as interchanging whole
+// rows at every step.  Every entry receives k_lu_band's operations in the
+// same order, so the factors and pivots are identical.  Needs
+// (kl+1) + (kl+ku+1) <= 1024 (one thread per entering entry).
 constexpr size_t kLuWindowSmemMax = 220 * 1024;
 __host__ __device__ inline size_t lu_window_smem(int n, int kl, int ku) {
-    return sizeof(double) * ((size_t)(kl + 1) * (kl + ku + 1) + kl + (kl + ku) + 64) + sizeof(int) * ((size_t)n + 64);
+    return sizeof(double) * ((size_t)(kl + 1) * (kl + ku + 1) + kl + (kl + ku) + 2) + sizeof(int) * ((size_t)n + 8);
 }
 
 static __global__ void __launch_bounds__(1024) k_lu_window(double* __restrict__ M, int n, int kl, int ku,
                                                            int* __restrict__ piv, int* __restrict__ info) {
     extern __shared__ double smem[];
     const int RW = kl + 1, CW = kl + ku + 1;
-    double* W = smem;
-    double* sL = W + (size_t)RW * CW;
-    double* sU = sL + kl;
-    double* wv = sU + (kl + ku);
-    int* rowfirst = reinterpret_cast<int*>(wv + 64);
-    int* wi = rowfirst + n;
-    int* s_p = wi + 32;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-    auto at = [&](int i, int c) -> double& { return W[(i % RW) * CW + (c % CW)]; };
+    double* W = smem;                                    // (i, c) at W[slot(c) * RW + slot(i)]
+    double* sL = W + (size_t)RW * CW;                    // the step's multipliers, rows j+1..j+kl
+    double* sU = sL + kl;                                // the step's pivot row, columns j+1..j+kl+ku
+    double* sv = sU + (kl + ku);                         // [0] the pivot, [1] the diagonal entry before the interchange
+    int* pv = reinterpret_cast<int*>(sv + 2);            // pivot row of every step
+    int* sp = pv + n;                                    // [0] the step's pivot row
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     if (tid == 0) info[0] = 0;
     for (int e = tid; e < RW * CW; e += blockDim.x) {
-        int r = e / CW, c = e % CW;
+        const int c = e / RW, r = e - c * RW;  // at j = 0 slot = index
         W[e] = (r < n && c < n) ? M[r + (long)c * n] : 0.0;
     }
-    for (int i = tid; i < n; i += blockDim.x) rowfirst[i] = i > kl ? i - kl : 0;
     __syncthreads();
-    for (int j = 0; j < n; j++) {
+    // Pivot search of column j by warp 0 (rows j..j+R, slots from rs).
+    auto pivot = [&](int j, int rs, int cs) {
         const int R = min(n - 1, j + kl) - j;
-        const int C = min(n - 1, j + kl + ku) - j;
-        // The row and column that enter the window after this step hold
-        // original matrix values (no step has touched them yet): load them
-        // now, so that the load latency overlaps the step.
-        const int nr = j + kl + 1, nc = j + kl + ku + 1;
-        double pre_r = 0.0, pre_c = 0.0;
-        const int cr = j + 1 + tid, ic = j + 1 + tid;  // thread tid: one entry of each
-        const bool has_r = nr < n && cr <= nc && cr < n, has_c = nc < n && ic < nr && ic < n;
-        if (has_r) pre_r = M[nr + (long)cr * n];
-        if (has_c) pre_c = M[ic + (long)nc * n];
         double bv = -1.0;
         int bi = n;
-        for (int i = j + tid; i <= j + R; i += blockDim.x) lu_better(fabs(at(i, j)), i, bv, bi);
+        for (int a = lane; a <= R; a += 32) {
+            int s = rs + a;
+            if (s >= RW) s -= RW;
+            lu_better(fabs(W[(size_t)cs * RW + s]), j + a, bv, bi);
+        }
         for (int o = 16; o > 0; o >>= 1) {
-            double ov = __shfl_down_sync(0xffffffffu, bv, o);
-            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
             lu_better(ov, oi, bv, bi);
         }
-        if (lane == 0) { wv[w] = bv; wi[w] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            for (int q = 1; q < nw; q++) lu_better(wv[q], wi[q], wv[0], wi[0]);
-            int p = wi[0] < n ? wi[0] : j;
-            *s_p = p;
+        if (lane == 0) {
+            const int p = bi < n ? bi : j;
+            int ps = rs + (p - j);
+            if (ps >= RW) ps -= RW;
+            sp[0] = p;
+            sv[0] = W[(size_t)cs * RW + ps];
+            sv[1] = W[(size_t)cs * RW + rs];
+            pv[j] = p;
             piv[j] = p + 1;
         }
-        __syncthreads();
-        const int p = *s_p;
-        const double apj = at(p, j);
+    };
+    if (warp == 0) pivot(0, 0, 0);
+    __syncthreads();
+    int rs0 = 0, cs0 = 0;  // slots of row j and column j
+    for (int j = 0; j < n; j++) {
+        const int R = min(n - 1, j + kl) - j, C = min(n - 1, j + kl + ku) - j;
+        // The row and column entering after this step hold original values:
+        // load them now (thread t < CW: entering row, column j+1+t; thread
+        // CW + t, t < RW: entering column, row j+1+t).
+        const int nr = j + kl + 1, ncl = j + kl + ku + 1;
+        double ent = 0.0;
+        bool has_ent = false;
+        if (tid < CW) {
+            const int c = j + 1 + tid;
+            has_ent = nr < n && c < n;
+            if (has_ent) ent = M[nr + (long)c * n];
+        } else if (tid < CW + RW) {
+            const int r = j + 1 + (tid - CW);
+            has_ent = ncl < n && r < n;
+            if (has_ent) ent = M[r + (long)ncl * n];
+        }
+        // (Read from the pivot search's copies: this phase rewrites both
+        // entries of the matrix window.)
+        const int p = sp[0];
+        int ps = rs0 + (p - j);
+        if (ps >= RW) ps -= RW;
+        const double apj = sv[0], ajj = sv[1];
         if (apj != 0.0) {
-            if (p != j) {
-                for (int c = j + tid; c <= j + C; c += blockDim.x) {
-                    double a = at(j, c);
-                    at(j, c) = at(p, c);
-                    at(p, c) = a;
+            const double rinv = 1.0 / apj;
+            if (tid < C) {
+                // column j+1+tid: interchange rows j and p; the pivot row
+                // (now row j) is final.
+                int cs = cs0 + 1 + tid;
+                if (cs >= CW) cs -= CW;
+                double* col = W + (size_t)cs * RW;
+                const double a = col[rs0], b = col[ps];
+                if (p != j) {
+                    col[rs0] = b;
+                    col[ps] = a;
                 }
-                const int lo = min(rowfirst[j], rowfirst[p]);
-                for (int c = lo + tid; c < j; c += blockDim.x) {
-                    double a = M[j + (long)c * n], b2 = M[p + (long)c * n];
-                    M[j + (long)c * n] = b2;
-                    M[p + (long)c * n] = a;
-                }
-                __syncthreads();
-                if (tid == 0) {
-                    int t = rowfirst[j];
-                    rowfirst[j] = rowfirst[p];
-                    rowfirst[p] = t;
-                }
-            }
-            __syncthreads();
-            const double r = 1.0 / at(j, j);
-            for (int i = tid; i < R; i += blockDim.x) {
-                double v = __dmul_rn(at(j + 1 + i, j), r);
-                at(j + 1 + i, j) = v;
-                sL[i] = v;
+                sU[tid] = b;
+                M[j + (long)(j + 1 + tid) * n] = b;
+            } else if (tid < C + R) {
+                // row j+1+a of column j: the multiplier (row p holds the old
+                // row j's entry after the interchange).
+                const int a = tid - C;
+                int s = rs0 + 1 + a;
+                if (s >= RW) s -= RW;
+                const double v = __dmul_rn(j + 1 + a == p ? ajj : W[(size_t)cs0 * RW + s], rinv);
+                W[(size_t)cs0 * RW + s] = v;
+                sL[a] = v;
+                M[(j + 1 + a) + (long)j * n] = v;
+            } else if (tid == C + R) {
+                W[(size_t)cs0 * RW + rs0] = apj;
+                M[j + (long)j * n] = apj;
             }
         } else {
+            // Zero pivot (the whole column is zero): no interchange, no
+            // scaling, info records the first one.
             if (tid == 0 && info[0] == 0) info[0] = j + 1;
-            for (int i = tid; i < R; i += blockDim.x) sL[i] = at(j + 1 + i, j);
-        }
-        for (int k = tid; k < C; k += blockDim.x) sU[k] = at(j, j + 1 + k);
-        __syncthreads();
-        for (int q = tid; q < R * C; q += blockDim.x) {
-            int ii = q % R, kk = q / R;
-            double u = sU[kk];
-            if (u != 0.0) {
-                double& a = at(j + 1 + ii, j + 1 + kk);
-                a = __dsub_rn(a, __dmul_rn(sL[ii], u));
+            if (tid < C) {
+                int cs = cs0 + 1 + tid;
+                if (cs >= CW) cs -= CW;
+                const double b = W[(size_t)cs * RW + rs0];
+                sU[tid] = b;
+                M[j + (long)(j + 1 + tid) * n] = b;
+            } else if (tid < C + R) {
+                const int a = tid - C;
+                int s = rs0 + 1 + a;
+                if (s >= RW) s -= RW;
+                const double v = W[(size_t)cs0 * RW + s];
+                sL[a] = v;
+                M[(j + 1 + a) + (long)j * n] = v;
+            } else if (tid == C + R) {
+                M[j + (long)j * n] = ajj;
             }
         }
-        // Column j (rows j..j+R) and row j (columns j+1..j+C) are final.
-        for (int i = tid; i <= R; i += blockDim.x) M[(j + i) + (long)j * n] = at(j + i, j);
-        for (int k = tid; k < C; k += blockDim.x) M[j + (long)(j + 1 + k) * n] = sU[k];
         __syncthreads();
-        // Slide: row j+kl+1 takes row j's slots, column j+kl+ku+1 column j's
-        // (one entry per thread: kl+ku+1 <= blockDim.x, checked by the host).
-        if (has_r) at(nr, cr) = pre_r;
-        if (has_c) at(ic, nc) = pre_c;
+        // Rank-1 update of rows j+1..j+R, columns j+1..j+C (pivot-row
+        // entries that are zero skipped, as k_lu_band does).
+        {
+            double l[4];
+            int rsl[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int a = lane + 32 * k;
+                int s = rs0 + 1 + a;
+                if (s >= RW) s -= RW;
+                rsl[k] = s;
+                l[k] = a < R ? sL[a] : 0.0;
+            }
+            for (int t = warp; t < C; t += nwarps) {
+                const double u = sU[t];
+                if (u == 0.0) continue;
+                int cs = cs0 + 1 + t;
+                if (cs >= CW) cs -= CW;
+                double* col = W + (size_t)cs * RW;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (lane + 32 * k < R) col[rsl[k]] = __dsub_rn(col[rsl[k]], __dmul_rn(l[k], u));
+            }
+        }
+        // The entering row takes row j's slot, the entering column column
+        // j's; neither slot is read by this step's update.
+        if (has_ent) {
+            if (tid < CW) {
+                int cs = cs0 + 1 + tid;
+                if (cs >= CW) cs -= CW;
+                W[(size_t)cs * RW + rs0] = ent;
+            } else {
+                int s = rs0 + 1 + (tid - CW);
+                if (s >= RW) s -= RW;
+                W[(size_t)cs0 * RW + s] = ent;
+            }
+        }
+        int rs1 = rs0 + 1, cs1 = cs0 + 1;
+        if (rs1 >= RW) rs1 = 0;
+        if (cs1 >= CW) cs1 = 0;
+        if (warp == 0 && j + 1 < n) {
+            // Column j+1 was updated by this warp (t = 0) and its entering
+            // entry written by lane 0.
+            __syncwarp();
+            pivot(j + 1, rs1, cs1);
+        }
+        rs0 = rs1;
+        cs0 = cs1;
         __syncthreads();
     }
+    // The interchanges of steps after j applied to column j's multipliers,
+    // in step order.
+    for (int c = tid; c < n; c += blockDim.x)
+        for (int j = c + 1; j < n; j++) {
+            const int p = pv[j];
+            if (p != j) {
+                const double a = M[j + (long)c * n];
+                M[j + (long)c * n] = M[p + (long)c * n];
+                M[p + (long)c * n] = a;
+            }
+        }
 }
 
 }  // namespace pgmg

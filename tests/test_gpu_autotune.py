@@ -281,3 +281,55 @@ def test_gs_l2_prefetch_bitwise(precision):
     A.solve(1e-10, 100, 0)
     B.solve(1e-10, 100, 0)
     assert np.array_equal(A.get_x(0), B.get_x(0))
+
+
+def _pivoting_problem(m, n, o, seed):
+    """Random 27-point stencils (boxes cropped at the grid's faces) whose
+    diagonal is small against the rest, so that partial pivoting interchanges
+    rows at most steps of the coarse LU."""
+    rng = np.random.default_rng(seed)
+    N = m * n * o
+    k, j, i = np.meshgrid(np.arange(o), np.arange(n), np.arange(m), indexing="ij")
+    idx, size = [i.reshape(-1), j.reshape(-1), k.reshape(-1)], [m, n, o]
+    slots = np.arange(27)
+    d = np.stack([slots % 3 - 1, (slots // 3) % 3 - 1, slots // 9 - 1], 1)
+    S = np.zeros((N, 6), np.int32)
+    ok = np.ones((N, 27), bool)
+    for a in range(3):
+        lo = np.where(idx[a] > 0, -1, 0)
+        hi = np.where(idx[a] < size[a] - 1, 2, 1)
+        S[:, 2 * a], S[:, 2 * a + 1] = lo, hi
+        ok &= (d[None, :, a] >= lo[:, None]) & (d[None, :, a] < hi[:, None])
+    coef = rng.uniform(-1, 1, (N, 27))
+    coef[:, 13] *= 0.05
+    coef[~ok] = 0.0
+    return coef, S, rng.uniform(-1, 1, N)
+
+
+@pytest.mark.parametrize("mno", [(9, 9, 9), (10, 9, 8), (6, 7, 5)])
+def test_lu_window_pivoting(mno):
+    """Both coarse LU kernels on single-level problems whose factorisation
+    interchanges rows: the reference-order solve gives the same x bit for bit
+    (the window kernel applies the interchanges to the multipliers it has
+    already written at the end), and x solves the system."""
+    coef, S, r = _pivoting_problem(*mno, seed=sum(mno))
+    xs = []
+    for win in (0, 1):
+        G = P.Multigrid(*mno, coarse=P.COARSE_LU_EXACT, smoother=P.SMOOTH_LEX)
+        G.set_option(P.OPT_LU_WINDOW, win)
+        G.setup_matrices(coef, S)
+        G.setup_fields(r)
+        assert G.nlevels == 1 and G.lu_enabled
+        G.solve_exact()
+        xs.append(G.get_x(0))
+        G.close()
+    assert np.array_equal(xs[0], xs[1])
+    m, n, o = mno
+    N = m * n * o
+    A = np.zeros((N, N))
+    for p in range(N):
+        i, j, k = p % m, (p // m) % n, p // (m * n)
+        for s in range(27):
+            if coef[p, s] != 0.0:
+                A[p, (i + s % 3 - 1) + m * ((j + (s // 3) % 3 - 1) + n * (k + s // 9 - 1))] = coef[p, s]
+    assert np.abs(A @ xs[0] - r).max() < 1e-9 * np.abs(r).max() * max(1.0, np.abs(xs[0]).max())
