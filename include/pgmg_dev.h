@@ -218,7 +218,13 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           colour pass's stencils and sources into L2 with
  *                           bulk prefetches at the start of each pass; 0 =
  *                           off (default).  Same results.  No counterpart in
- *                           the reference. */
+ *                           the reference.
+ *   PGMG_OPT_LU_INVERSE_BAND 1 (default) = the explicit coarse inverse is
+ *                           computed one warp per column over the factors'
+ *                           band (where it is at most 256 rows on either side
+ *                           of the diagonal); 0 = one block per column over
+ *                           the dense factors.  Same inverse bit for bit.
+ *                           Takes effect at the next set-up. */
 enum {
     PGMG_OPT_GRAPHS = 1,
     PGMG_OPT_CLUSTER_FIRST = 2,
@@ -240,7 +246,8 @@ enum {
     PGMG_OPT_LU_WINDOW = 18,
     PGMG_OPT_GS_TMA = 19,
     PGMG_OPT_RAT_TILE = 20,
-    PGMG_OPT_GS_L2_PREFETCH = 21
+    PGMG_OPT_GS_L2_PREFETCH = 21,
+    PGMG_OPT_LU_INVERSE_BAND = 22
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after

@@ -42,6 +42,7 @@ OPT_LU_WINDOW = 18
 OPT_GS_TMA = 19
 OPT_RAT_TILE = 20
 OPT_GS_L2_PREFETCH = 21
+OPT_LU_INVERSE_BAND = 22
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",

@@ -349,7 +349,7 @@ pgmg_status restrict_level(pgmg_handle* h, int l) {
     if (F.g.prd)
         LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict<T, true>, F.g, Cl.g, vf.res, vc.r, vc.x);
     else
-        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict_fast<T>, F.g, Cl.g, vf.res, vc.r, vc.x);
+        LAUNCH(nblk(Cl.g.npts), kBlock, k_restrict_fast<T>, F.g, Cl.g, coarse_split(F.g, Cl.g), vf.res, vc.r, vc.x);
     return wrap_level<T>(h, l);
 }
 
@@ -706,17 +706,28 @@ pgmg_status lu_setup(pgmg_handle* h) {
         }
         CKL();
     }
-    int info = 0;
+    k_lu_extent<<<nblk(n * 32), kBlock, 0, h->stream>>>(h->M, (int)n, h->info + 1);
+    CKL();
+    int info4[4] = {0, 0, 0, 0};
     double u0 = 0, un = 0;
-    CK(cudaMemcpyAsync(&info, h->info, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(info4, h->info, sizeof(info4), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(&u0, h->M, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(&un, h->M + n * n - 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    const int info = info4[0], bl = info4[1], bu = info4[2];
     // Conditioning check of region_tr.cc:524-533.
     double hi = fabs(u0), lo = fabs(un);
     if (info != 0 || hi == 0 || lo / hi < 2.220446049250313e-16 * 1e4) return PGMG_OK;
     if (h->dims.coarse == PGMG_COARSE_LU) {
-        k_lu_inverse<<<(unsigned)n, 256, n * sizeof(double), h->stream>>>(h->M, h->piv, (int)n, h->Minv);
+        const unsigned nbk = (unsigned)((n + kInvWarps - 1) / kInvWarps);
+        const size_t ism = kInvWarps * n * sizeof(double);
+        if (h->lu_inv_band && bl <= 128 && bu <= 256) {
+            k_lu_inverse_band<4, 8><<<nbk, 32 * kInvWarps, ism, h->stream>>>(h->M, h->piv, (int)n, bl, bu, h->Minv);
+        } else if (h->lu_inv_band && bl <= 256 && bu <= 256) {
+            k_lu_inverse_band<8, 4><<<nbk, 32 * kInvWarps, ism, h->stream>>>(h->M, h->piv, (int)n, bl, bu, h->Minv);
+        } else {
+            k_lu_inverse<<<(unsigned)n, 256, n * sizeof(double), h->stream>>>(h->M, h->piv, (int)n, h->Minv);
+        }
         CKL();
     }
     h->lu_ok = 1;
@@ -753,13 +764,19 @@ pgmg_status prepare_device_kernels(int device) {
                    cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_rat_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRtSmem) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_rat_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRatSmem) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_lu_inverse_band<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kInvWarps * kMaxExact * sizeof(double))) == cudaSuccess;
+    ok = ok && cudaFuncSetAttribute(k_lu_inverse_band<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kInvWarps * kMaxExact * sizeof(double))) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)gs_tma_smem<double, 256>()) == cudaSuccess;
     ok = ok && cudaFuncSetAttribute(k_gs_colour_tma<float, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)gs_tma_smem<float, 256>()) == cudaSuccess;
     cudaFuncAttributes fa;
     const void* setup_kernels[] = {(const void*)k_gs_colour_tma<double, 128>, (const void*)k_gs_colour_tma<float, 128>,(const void*)k_lu_build,       (const void*)k_lu_band,
-                                   (const void*)k_lu_inverse,     (const void*)k_rat_bounds,
+                                   (const void*)k_lu_inverse,     (const void*)k_lu_inverse_band<4, 8>,
+                                   (const void*)k_lu_inverse_band<8, 4>,
+                                   (const void*)k_lu_extent,      (const void*)k_rat_bounds,
                                    (const void*)k_rat_fill,       (const void*)k_rat_fill_small,
                                    (const void*)k_assemble_q1,    (const void*)k_rhs_uniform,
                                    (const void*)k_resrestrict<double, RrSmall>,
@@ -983,6 +1000,9 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_LU_WINDOW:
             h->lu_window = value != 0;
             break;
+        case PGMG_OPT_LU_INVERSE_BAND:
+            h->lu_inv_band = value != 0;
+            break;
         case PGMG_OPT_GS_TMA:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_tma must be >= 0");
             h->gs_tma = value;
@@ -1047,6 +1067,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_COARSE_SHARED: *value = h->coarse_shared; return PGMG_OK;
         case PGMG_OPT_FUSED_RESTRICT: *value = h->fused_restrict; return PGMG_OK;
         case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
+        case PGMG_OPT_LU_INVERSE_BAND: *value = h->lu_inv_band; return PGMG_OK;
         case PGMG_OPT_GS_TMA: *value = h->gs_tma; return PGMG_OK;
         case PGMG_OPT_RAT_TILE: *value = h->rat_tile; return PGMG_OK;
         case PGMG_OPT_GS_L2_PREFETCH: *value = h->gs_l2pf; return PGMG_OK;
@@ -1184,7 +1205,8 @@ pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
             dim3 grid((unsigned)((Cl.g.m + kRtX - 1) / kRtX), (unsigned)Cl.g.n, (unsigned)((Cl.g.o + kRtKC - 1) / kRtKC));
             k_rat_tile<<<grid, kRtThreads, kRtSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
         } else {
-            k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, kRatSmem, h->stream>>>(F.g, Cl.g, F.A64, F.S, Cl.A64);
+            k_rat_fill<<<nblk(Cl.g.npts, kRatBlock), kRatBlock, kRatSmem, h->stream>>>(F.g, Cl.g, coarse_split(F.g, Cl.g),
+                                                                                      F.A64, F.S, Cl.A64);
         }
         CKL();
     }

@@ -171,6 +171,9 @@ struct pgmg_handle {
     // The coarse LU factorises in a shared-memory band window (k_lu_window)
     // where it fits, instead of the one-block kernel on device memory.
     bool lu_window = true;
+    // The explicit coarse inverse one warp per column over the factors' band
+    // (k_lu_inverse_band) where the band allows, instead of k_lu_inverse.
+    bool lu_inv_band = true;
     // Galerkin operators of large non-periodic levels by k_rat_tile (one
     // thread per coarse point and slot) instead of k_rat_fill (off: measured
     // slower).

@@ -600,9 +600,18 @@ __global__ void __launch_bounds__(kBlock) k_interp_cube(LevelGeom gf, LevelGeom 
 // same contributions in the same order, all 27 loads issued first); the
 // others take restrict_sum itself.
 template <class T, class Get>
+__device__ __forceinline__ T restrict_inner_sum(int I, int J, int K, Get res);
+
+template <class T, class Get>
 __device__ __forceinline__ T restrict_fast_sum(const LevelGeom& gf, int I, int J, int K, Get res) {
     if (!(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o)))
         return restrict_sum<T, false>(gf, I, J, K, res);
+    return restrict_inner_sum<T>(I, J, K, res);
+}
+
+// restrict_sum of a coarse point interior on every axis (inner_axis).
+template <class T, class Get>
+__device__ __forceinline__ T restrict_inner_sum(int I, int J, int K, Get res) {
     // Per axis: cube a (0: I-1, 1: I), role d -> fine offset 2a+d-2 from 2I,
     // weight 0 (not visited), 1/2, 1, 1/2.
     T rv[27];
@@ -645,11 +654,23 @@ __device__ __forceinline__ void restrict_fast_at(const LevelGeom& gf, const Leve
     xc[gc.xi(I, J, K)] = T(0);
 }
 
+// Restriction of a non-periodic level, interior coarse points first (see
+// CoarseSplit): their sums run with the weights known at compile time, the
+// shell's take restrict_sum.
 template <class T>
-__global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeom gc, const T* __restrict__ res,
-                                                          T* __restrict__ rc, T* __restrict__ xc) {
+__global__ void __launch_bounds__(kBlock) k_restrict_fast(LevelGeom gf, LevelGeom gc, CoarseSplit sp,
+                                                          const T* __restrict__ res, T* __restrict__ rc,
+                                                          T* __restrict__ xc) {
     pdl_enter();
-    restrict_fast_at<T>(gf, gc, res, rc, xc, blockIdx.x * (long)blockDim.x + threadIdx.x);
+    long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= gc.npts) return;
+    auto get = [&](int i, int j, int k) { return res[gf.ri(i, j, k)]; };
+    int I, J, K;
+    if (split_point(gc, sp, q, I, J, K))
+        rc[gc.ri(I, J, K)] = restrict_inner_sum<T>(I, J, K, get);
+    else
+        rc[gc.ri(I, J, K)] = restrict_sum<T, false>(gf, I, J, K, get);
+    xc[gc.xi(I, J, K)] = T(0);
 }
 
 // Residual fused with the restriction of a non-periodic level

@@ -235,12 +235,11 @@ __device__ __forceinline__ void rat_fast_step(int n, const LevelGeom& gf, const 
     if constexpr (N + 1 < 27) rat_fast_step<N + 1>(n, gf, Af, I, J, K, acc);
 }
 
-// Whether coarse point (I,J,K) takes the interior gather: non-periodic
-// level, interior on every axis, all 27 fine boxes [-1,2)^3 (each box is six
-// int8 at an even offset, read as three 16-bit words (lo, hi) = (-1, 2)).
-__device__ __forceinline__ bool rat_interior(const LevelGeom& gf, const int8_t* __restrict__ Sf, int I, int J,
-                                             int K) {
-    if (gf.prd || !(inner_axis(I, gf.m) && inner_axis(J, gf.n) && inner_axis(K, gf.o))) return false;
+// Whether an interior coarse point (I,J,K) (CoarseSplit) takes the interior
+// gather: all 27 fine boxes [-1,2)^3 (each box is six int8 at an even
+// offset, read as three 16-bit words (lo, hi) = (-1, 2)).
+__device__ __forceinline__ bool rat_full_boxes(const LevelGeom& gf, const int8_t* __restrict__ Sf, int I, int J,
+                                               int K) {
     bool full = true;
 #pragma unroll
     for (int oz = -1; oz <= 1; oz++)
@@ -255,23 +254,26 @@ __device__ __forceinline__ bool rat_interior(const LevelGeom& gf, const int8_t* 
     return full;
 }
 
-// The block's interior points walk the 27 fine points in lock step
-// (a barrier after each), so that the warps of an SM run one fine point's
-// code at a time: unrolled, the 27 fine points are ~100 KB of instructions,
-// which warps at different fine points would keep evicting from the
-// instruction cache.  The block's other points take rat_general afterwards.
+// Coarse points in CoarseSplit order: the interior box first, whose blocks
+// walk the 27 fine points in lock step (a barrier after each), so that the
+// warps of an SM run one fine point's code at a time -- unrolled, the 27
+// fine points are ~100 KB of instructions, which warps at different fine
+// points would keep evicting from the instruction cache -- then the shell,
+// whose points take rat_general in warps of their own (mixed into interior
+// warps, one boundary point made its whole warp wait for the general path).
 // Dynamic shared memory: kRatSmem (the accumulators or the coefficient
 // columns, one column of 27 per thread).
 constexpr size_t kRatSmem = 27 * kRatBlock * sizeof(double);
 
-static __global__ void __launch_bounds__(kRatBlock, 2) k_rat_fill(LevelGeom gf, LevelGeom gc, const double* __restrict__ Af,
+static __global__ void __launch_bounds__(kRatBlock, 2) k_rat_fill(LevelGeom gf, LevelGeom gc, CoarseSplit sp,
+                                                        const double* __restrict__ Af,
                                                         const int8_t* __restrict__ Sf, double* __restrict__ Ac) {
     extern __shared__ double sa[];
     const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const bool valid = q < gc.npts;
     int I = 0, J = 0, K = 0;
-    if (valid) decode_nat(gc, q, I, J, K);
-    const bool fast = valid && rat_interior(gf, Sf, I, J, K);
+    const bool inner = valid && split_point(gc, sp, q, I, J, K);
+    const bool fast = inner && rat_full_boxes(gf, Sf, I, J, K);
     double* col = sa + threadIdx.x;  // this thread's column: element s at col[s * kRatBlock]
     double* out = nullptr;
     if (valid) out = Ac + (long)gc.colour(I, J, K) * 27 * gc.Nc + gc.cidx(I, J, K);
@@ -569,6 +571,122 @@ static __global__ void __launch_bounds__(256) k_lu_inverse(const double* __restr
         }
         if (threadIdx.x == 0) Minv[(long)j * n + c] = xj;
         __syncthreads();
+    }
+}
+
+// Widest extent of the factors' non-zeros off the diagonal, for
+// k_lu_inverse_band: ext[0] = max over columns j of (last row i > j with
+// M(i,j) != 0) - j, ext[1] = max of j - (first row i < j with M(i,j) != 0);
+// ext zeroed by the caller.  One warp per column.
+static __global__ void __launch_bounds__(256) k_lu_extent(const double* __restrict__ M, int n, int* __restrict__ ext) {
+    const int j = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (j >= n) return;
+    int lo = 0, up = 0;
+    const double* col = M + (long)j * n;
+    for (int i = lane; i < n; i += 32)
+        if (col[i] != 0.0) {
+            if (i > j) lo = max(lo, i - j);
+            else if (i < j) up = max(up, j - i);
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = max(lo, __shfl_down_sync(0xffffffffu, lo, o));
+        up = max(up, __shfl_down_sync(0xffffffffu, up, o));
+    }
+    if (lane == 0) {
+        atomicMax(ext, lo);
+        atomicMax(ext + 1, up);
+    }
+}
+
+// k_lu_inverse with one warp per column and the factors' band: at forward
+// step j the entries below j within bl rows, at backward step j those above
+// within bu rows (k_lu_extent; everything beyond is zero, and an update by a
+// zero factor entry changes no bit of a solution entry, which can never be
+// -0 here), each entry receiving the same operations in the same order as in
+// k_lu_inverse -- the same inverse bit for bit.  A warp works through its
+// column without block barriers, loading the factor entries of several steps
+// at once so that their L2 latency is paid once per group of steps; the
+// 729 columns of a 9^3 level run as 729 concurrent warps.  A lane holds RL
+// rows of the forward band (bl <= 32 RL) for GF steps at a time and 8 rows
+// of the backward band (bu <= 256) for 4 steps.  Dynamic shared memory:
+// kInvWarps columns of n doubles.
+constexpr int kInvWarps = 4;
+constexpr int kInvGroupB = 4;
+
+template <int RL, int GF>
+__global__ void __launch_bounds__(32 * kInvWarps) k_lu_inverse_band(const double* __restrict__ M,
+                                                                      const int* __restrict__ piv, int n, int bl,
+                                                                      int bu, double* __restrict__ Minv) {
+    extern __shared__ double Xs[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kInvWarps + w;
+    if (c >= n) return;  // a whole warp; no block barrier follows
+    double* X = Xs + (size_t)w * n;
+    for (int i = lane; i < n; i += 32) X[i] = i == c ? 1.0 : 0.0;
+    __syncwarp();
+    if (lane == 0)
+        for (int i = 0; i < n; i++) {
+            const int p = piv[i] - 1;
+            if (p != i) {
+                const double t = X[i];
+                X[i] = X[p];
+                X[p] = t;
+            }
+        }
+    __syncwarp();
+    for (int j0 = 0; j0 < n; j0 += GF) {
+        double Lb[GF][RL];
+#pragma unroll
+        for (int s = 0; s < GF; s++)
+#pragma unroll
+            for (int k = 0; k < RL; k++) {
+                const int j = j0 + s, a = lane + 32 * k, i = j + 1 + a;
+                Lb[s][k] = (j < n && a < bl && i < n) ? M[i + (long)j * n] : 0.0;
+            }
+#pragma unroll
+        for (int s = 0; s < GF; s++) {
+            const int j = j0 + s;
+            if (j < n) {
+                const double xj = X[j];
+                if (xj != 0.0)
+#pragma unroll
+                    for (int k = 0; k < RL; k++) {
+                        const int a = lane + 32 * k, i = j + 1 + a;
+                        if (a < bl && i < n) X[i] = __dsub_rn(X[i], __dmul_rn(xj, Lb[s][k]));
+                    }
+            }
+            __syncwarp();
+        }
+    }
+    for (int j0 = n - 1; j0 >= 0; j0 -= kInvGroupB) {
+        double Ub[kInvGroupB][8], dg[kInvGroupB];
+#pragma unroll
+        for (int s = 0; s < kInvGroupB; s++) {
+            const int j = j0 - s;
+            dg[s] = j >= 0 ? M[j + (long)j * n] : 1.0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int a = lane + 32 * k, i = j - 1 - a;
+                Ub[s][k] = (j >= 0 && a < bu && i >= 0) ? M[i + (long)j * n] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < kInvGroupB; s++) {
+            const int j = j0 - s;
+            if (j >= 0) {
+                double xj = X[j];
+                if (xj != 0.0) {
+                    xj = xj / dg[s];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int a = lane + 32 * k, i = j - 1 - a;
+                        if (a < bu && i >= 0) X[i] = __dsub_rn(X[i], __dmul_rn(xj, Ub[s][k]));
+                    }
+                }
+                if (lane == 0) Minv[(long)j * n + c] = xj;
+            }
+            __syncwarp();
+        }
     }
 }
 

@@ -333,3 +333,54 @@ def test_lu_window_pivoting(mno):
             if coef[p, s] != 0.0:
                 A[p, (i + s % 3 - 1) + m * ((j + (s // 3) % 3 - 1) + n * (k + s // 9 - 1))] = coef[p, s]
     assert np.abs(A @ xs[0] - r).max() < 1e-9 * np.abs(r).max() * max(1.0, np.abs(xs[0]).max())
+
+
+def _weak_rows_problem(m, n, o, seed, nweak=8):
+    """Diagonally dominant random stencils with a few rows whose diagonal is
+    tiny: the LU interchanges rows at some two dozen steps, and the factors
+    stay within a band of about 100 (small grids)."""
+    rng = np.random.default_rng(seed)
+    coef, S, _ = _pivoting_problem(m, n, o, seed)
+    ok = coef != 0.0
+    ok[:, 13] = True
+    coef = rng.uniform(-1, 1, coef.shape) * 0.1
+    coef[:, 13] = 4.0
+    coef[rng.choice(coef.shape[0], nweak, replace=False), 13] = 1e-3
+    coef[~ok] = 0.0
+    return coef, S, rng.uniform(-1, 1, coef.shape[0])
+
+
+@pytest.mark.parametrize("case", ["q1_33", "q1_65", "q1_20x33x9", "weak_4x5x6", "weak_5", "weak_6x5x4",
+                                  "weak_8x6x7", "weak_7x6x5", "pivot_9"])
+def test_lu_inverse_band_same_inverse(case):
+    """The explicit coarse inverse computed one warp per column over the
+    factors' band equals the one-block-per-column dense computation bit for
+    bit: the coarse solves, and so the V-cycles, agree exactly (Q1 problems;
+    single-level problems whose LU interchanges rows at a few steps, with the
+    factors still banded; and one with interchanges at most steps, whose
+    factors are not banded, where both take the dense kernel)."""
+    if case.startswith("q1"):
+        mno = {"q1_33": (33, 33, 33), "q1_65": (65, 65, 65), "q1_20x33x9": (20, 33, 9)}[case]
+        coef, S, r = q1_problem(*mno, sigma=1.5, seed=7)
+    elif case.startswith("weak"):
+        # band below the diagonal 87, 81, 74 (4 rows per lane); 161, 140 (8)
+        mno = {"weak_4x5x6": (4, 5, 6), "weak_5": (5, 5, 5), "weak_6x5x4": (6, 5, 4), "weak_8x6x7": (8, 6, 7),
+               "weak_7x6x5": (7, 6, 5)}[case]
+        coef, S, r = _weak_rows_problem(*mno, seed=5)
+    else:
+        coef, S, r = _pivoting_problem(9, 9, 9, seed=28)
+        mno = (9, 9, 9)
+    hs = []
+    for band in (0, 1):
+        G = P.Multigrid(*mno, coarse=P.COARSE_LU, smoother=P.SMOOTH_LEX)
+        G.set_option(P.OPT_LU_INVERSE_BAND, band)
+        G.setup_matrices(coef, S)
+        G.setup_fields(r)
+        assert G.lu_enabled
+        hs.append(G)
+    for _ in range(3):
+        for G in hs:
+            G.v_cycle(0)
+        assert np.array_equal(hs[0].get_x(0), hs[1].get_x(0))
+    for G in hs:
+        G.close()
