@@ -16,9 +16,9 @@ FP32 V-cycles between FP64 residual checks the same way).
 Prints one JSON line (rank 0).  ``value`` is the device-timed s/solve with
 the operator and source resident in device memory (inputs > L2, so no flush
 is needed); ``e2e`` times the same solve through the C ABI from pinned host
-buffers (source up, solution down) every step.  Under torchrun every rank
-solves its own replica (independent problems; no collective on the data
-path) and the line reports the max over ranks.
+buffers (source up, solution down, pgmg_dev_solve_io) every step.  Under
+torchrun every rank solves its own replica (independent problems; no
+collective on the data path) and the line reports the max over ranks.
 """
 from __future__ import annotations
 
@@ -374,19 +374,16 @@ def run_ours(a):
     # --- end to end through the C ABI with pinned host buffers -------------
     hr = torch.from_numpy(r).pin_memory()
     hx = torch.empty(npts, dtype=torch.float64).pin_memory()
+    # pgmg_dev_solve_io: the source copied in, the solve, the solution copied
+    # out (its copy overlapping the final residual check), in one call.
     for _ in range(1):
-        G.set_field(0, P.FIELD_R, hr.data_ptr())
-        solve_once(G)
-        G.get_field(0, P.FIELD_X, hx.data_ptr())
+        G.solve_io(hr.data_ptr(), hx.data_ptr(), a.tol, 100, 0)
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(a.steps):
-        G.set_field(0, P.FIELD_R, hr.data_ptr())
-        G.clear_x(0)
-        G.solve(a.tol, 100, 0)
-        G.get_field(0, P.FIELD_X, hx.data_ptr())
+        G.solve_io(hr.data_ptr(), hx.data_ptr(), a.tol, 100, 0)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / a.steps)

@@ -427,9 +427,20 @@ pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle *h, double p_scale, int *result,
  * (>= 1; in mixed precision the FP32 V-cycles per refinement step), or 0 for
  * an adaptive schedule that predicts the remaining cycles from the observed
  * reduction factor (mixed precision: up to 16 cycles per step, and no more
- * than a 1e-5 predicted reduction).  Outputs may be NULL. */
+ * than a 1e-5 predicted reduction, 1e-6 while the solve gains more than a
+ * digit per cycle).  Outputs may be NULL. */
 pgmg_status pgmg_dev_solve_relres(pgmg_handle *h, double tol, int max_cycles, int check_every,
                                   int *cycles, double *relres);
+/* The whole solve from caller arrays (no counterpart in the reference): the
+ * level-0 source r (natural order) is uploaded, x set to zero, the solve run
+ * as pgmg_dev_solve_relres, and the solution written to x (natural order).
+ * The same iterates, cycle count and relative residual as set_field(R) +
+ * clear_x + solve_relres + get_field(X).  r and x may be host (pinned or
+ * pageable) or device memory; with pinned x the solution's copy overlaps the
+ * final residual check (it starts at a check that may end the solve; a later
+ * one replaces it if the solve continues).  Outputs may be NULL. */
+pgmg_status pgmg_dev_solve_io(pgmg_handle *h, const double *r, double *x, double tol, int max_cycles,
+                              int check_every, int *cycles, double *relres);
 
 /* ---- batched solves (many independent problems per launch) ------------- */
 

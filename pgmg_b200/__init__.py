@@ -114,6 +114,8 @@ SIGNATURES = [
     ("pgmg_dev_norms", C.c_int, [_VP, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pgmg_dev_solve_v_cycles", C.c_int, [_VP, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("pgmg_dev_solve_relres", C.c_int, [_VP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("pgmg_dev_solve_io", C.c_int, [_VP, _VP, _VP, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double)]),
     ("pgmg_batch_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     ("pgmg_batch_destroy", C.c_int, [_VP]),
     ("pgmg_batch_last_error", C.c_char_p, [_VP]),
@@ -537,6 +539,25 @@ class Multigrid:
         rr = C.c_double()
         self._ck(lib().pgmg_dev_solve_relres(self._h, tol, max_cycles, check_every, C.byref(cyc), C.byref(rr)),
                  "solve")
+        return cyc.value, rr.value
+
+    def solve_io(self, r, x_out, tol: float = 1e-10, max_cycles: int = 100, check_every: int = 1):
+        """The whole solve from caller arrays (pgmg_dev_solve_io): source r in,
+        solution written to x_out (natural order; numpy arrays or pointers,
+        host or device), x starting from zero."""
+        n = self.npts(0)
+        if not isinstance(r, int):
+            r = np.ascontiguousarray(r, np.float64)
+            if r.size != n:
+                raise ValueError("source size does not match level 0")
+        if not isinstance(x_out, int):
+            if x_out.dtype != np.float64 or not x_out.flags.c_contiguous or x_out.size != n:
+                raise ValueError("x_out must be a contiguous float64 array of level 0's size")
+        cyc = C.c_int()
+        rr = C.c_double()
+        self._ck(lib().pgmg_dev_solve_io(self._h, r if isinstance(r, int) else _ptr(r),
+                                         x_out if isinstance(x_out, int) else _ptr(x_out), tol, max_cycles,
+                                         check_every, C.byref(cyc), C.byref(rr)), "solve_io")
         return cyc.value, rr.value
 
 

@@ -935,6 +935,9 @@ pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
     if (h->norm_pin) cudaFreeHost(h->norm_pin);
     if (h->ev_pre) cudaEventDestroy(h->ev_pre);
     if (h->ev_post) cudaEventDestroy(h->ev_post);
+    if (h->ostream) cudaStreamSynchronize(h->ostream);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->ostream) cudaStreamDestroy(h->ostream);
     if (h->arena.base && h->own_arena) cudaFree(h->arena.base);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
@@ -1787,8 +1790,14 @@ struct CheckPlan {
 };
 
 
-pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
-                                  double* relres) {
+// The solve of pgmg_dev_solve_relres.  x_out (pgmg_dev_solve_io; may be
+// NULL): the caller's buffer for the level-0 solution in natural order.  At
+// a check that may end the solve the solution is converted and copied there
+// on the handle's output stream while the check itself runs on the handle's
+// stream; if the check does not end the solve, a later copy on the same
+// stream follows the stale one.
+static pgmg_status solve_core(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
+                              double* relres, double* x_out) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (check_every < 0) check_every = 1;
@@ -1802,12 +1811,32 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
     dim3 grid((unsigned)(8 * nblk((long)g.M2 * g.N2 * g.O2)));  // colours interleaved
     long nb = nblk((long)g.M2 * g.N2 * g.O2) * 8;
     bool mixed = h->dims.precision == PGMG_MIXED;
+    bool spec64 = false, out_now = false;
     plan.rho0 = h->last_rho;
     for (;;) {
         // Mixed precision computes the FP64 residual at every refinement step
         // (it is the next correction's source), so it checks every step too.
         bool check = mixed || nc >= next_check || nc >= max_cycles;
         bool zero = nc == 0 && h->x0_zero;  // residual = source: no stencil pass needed
+        out_now = false;
+        if (x_out && check && !zero) {
+            // An FP64 check is scheduled where the solve is predicted to
+            // converge; a mixed one ends the solve unless its predicted
+            // residual is above kSlack * tol.
+            bool more = false;
+            if (mixed) {
+                double q = plan.rho();
+                more = q > 0 && q < 0.9 && plan.last_r > 0 && plan.last_r * pow(q, nc - plan.last_n) > kSlack * tol;
+            }
+            if (!more) {
+                CK(cudaEventRecord(h->ev_out, h->stream));
+                CK(cudaStreamWaitEvent(h->ostream, h->ev_out, 0));
+                k_x_to_nat<double><<<nblk(g.npts), kBlock, 0, h->ostream>>>(g, L0.x64, h->stage);
+                CKL();
+                CK(cudaMemcpyAsync(x_out, h->stage, sizeof(double) * g.npts, cudaMemcpyDefault, h->ostream));
+                out_now = true;
+            }
+        }
         if (check) TRY(check_begin(h));
         if (zero) {
             if (mixed || check) {
@@ -1847,13 +1876,26 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             }
             TRY(read_norms(h));
         } else if (check) {
-            TRY(reduce_and_read(h, nb));
+            // FP64 from x = 0: the check is the source norm, which ends the
+            // solve only for a zero or non-finite source (or tol >= 1), so
+            // the first V-cycle is enqueued before the host waits for it;
+            // when the solve does end there, x is cleared again.
+            TRY(reduce_launch(h, nb));
+            if (zero && nc < max_cycles && tol < 1.0) {
+                TRY(run_vcycle<double>(h, 0, smoother));
+                spec64 = true;
+            }
+            TRY(read_norms(h));
         }
         if (check) {
             res2 = h->norm_host[0];
             rhs2 = h->norm_host[1];
             rr = rhs2 > 0 ? sqrt(res2 / rhs2) : sqrt(res2);
-            if (std::isnan(rr) || rr < tol || nc >= max_cycles) break;
+            if (std::isnan(rr) || rr < tol || nc >= max_cycles) {
+                if (spec64) TRY(pgmg_dev_clear_x(h, 0));
+                if (spec64) out_now = false;
+                break;
+            }
             plan.record(nc, rr);
             next_check = plan.next(nc, tol);
             if (next_check > max_cycles) next_check = max_cycles;
@@ -1878,6 +1920,8 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
             TRY(wrap_level<double>(h, 0));
             nc += inner;
             continue;
+        } else if (spec64) {
+            spec64 = false;  // this cycle was enqueued before the check was read
         } else {
             TRY(run_vcycle<double>(h, 0, smoother));
         }
@@ -1891,9 +1935,45 @@ pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, in
         double q = pow(rr / plan.first_r, 1.0 / (nc - plan.first_n));
         if (q > 0 && q < 0.9) h->last_rho = q;
     }
+    if (x_out) {
+        // The copy enqueued at the final check holds the final x; otherwise
+        // (the solve ended at x = 0, or without a copy) copy it now.
+        CK(cudaStreamSynchronize(h->ostream));
+        if (!out_now) {
+            k_x_to_nat<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, L0.x64, h->stage);
+            CKL();
+            CK(cudaMemcpyAsync(x_out, h->stage, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+    }
     if (cycles) *cycles = nc;
     if (relres) *relres = rr;
     return check_grid(h);
+}
+
+pgmg_status pgmg_dev_solve_relres(pgmg_handle* h, double tol, int max_cycles, int check_every, int* cycles,
+                                  double* relres) {
+    return solve_core(h, tol, max_cycles, check_every, cycles, relres, nullptr);
+}
+
+pgmg_status pgmg_dev_solve_io(pgmg_handle* h, const double* r, double* x, double tol, int max_cycles,
+                              int check_every, int* cycles, double* relres) {
+    if (!h || !r || !x) return PGMG_ERR_ARG;
+    if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    if (!h->ostream) {
+        if (cudaStreamCreateWithFlags(&h->ostream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(h, PGMG_ERR_CUDA, "output stream");
+        }
+    }
+    Level& L0 = h->L[0];
+    const LevelGeom& g = L0.g;
+    CK(cudaMemcpyAsync(h->stage, r, sizeof(double) * g.npts, cudaMemcpyDefault, h->stream));
+    k_nat_to_cm<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L0.r64);
+    CKL();
+    TRY(pgmg_dev_clear_x(h, 0));
+    return solve_core(h, tol, max_cycles, check_every, cycles, relres, x);
 }
 
 }  // extern "C"

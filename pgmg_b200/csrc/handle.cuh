@@ -137,6 +137,10 @@ struct pgmg_handle {
     // ev_post after the reduction.
     double* norm_pin = nullptr;
     cudaEvent_t ev_pre = nullptr, ev_post = nullptr;
+    // pgmg_dev_solve_io: the solution's copy to the caller's buffer runs on
+    // ostream (created at the first call), after ev_out on the handle's stream.
+    cudaStream_t ostream = nullptr;
+    cudaEvent_t ev_out = nullptr;
     bool own_arena = true;         // false: memory given by the caller
     // mg_guide state (multigrid.hh:34-118)
     int period = 16, iter = 16, use_avg = 0, tol_set = 0;
