@@ -779,6 +779,7 @@ pgmg_status prepare_device_kernels(int device) {
                                    (const void*)k_lu_extent,      (const void*)k_rat_bounds,
                                    (const void*)k_rat_fill,       (const void*)k_rat_fill_small,
                                    (const void*)k_assemble_q1,    (const void*)k_rhs_uniform,
+                                   (const void*)k_cell_exp,
                                    (const void*)k_resrestrict<double, RrSmall>,
                                    (const void*)k_resrestrict<float, RrSmall>};
     for (const void* k : setup_kernels) ok = ok && cudaFuncGetAttributes(&fa, k) == cudaSuccess;
@@ -1173,6 +1174,15 @@ pgmg_status pgmg_dev_assemble_q1(pgmg_handle* h, const double* cells, int from_l
             CK(cudaMemcpyAsync(h->stage, cells, nc * sizeof(double), cudaMemcpyHostToDevice, h->stream));
             dc = h->stage;
         }
+    }
+    if (dc && from_log) {
+        // kappa of every cell once, into the level's residual scratch (free
+        // during set-up; at least npts > cells doubles).
+        size_t nc = (size_t)(g.m - 1) * (g.n - 1) * (g.o - 1);
+        k_cell_exp<<<nblk((long)nc), kBlock, 0, h->stream>>>(dc, (long)nc, sigma, L.res64);
+        CKL();
+        dc = L.res64;
+        from_log = 0;
     }
     int mx = g.m > g.n ? (g.m > g.o ? g.m : g.o) : (g.n > g.o ? g.n : g.o);
     double hh = 1.0 / (double)(mx - 1);

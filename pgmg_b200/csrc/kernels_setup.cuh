@@ -769,6 +769,16 @@ __device__ __forceinline__ double cell_kappa(const double* c, long idx, int from
     return from_log ? exp(sigma * c[idx]) : c[idx];
 }
 
+// kappa = exp(sigma * g) of every cell, once: k_assemble_q1 reads each
+// cell's kappa from its 8 corner points, and evaluating the exponential
+// there 8 times over bounded that kernel.  The same expression, so the
+// same values as cell_kappa's.
+static __global__ void __launch_bounds__(256) k_cell_exp(const double* __restrict__ g, long n, double sigma,
+                                                         double* __restrict__ kap) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) kap[i] = exp(sigma * g[i]);
+}
+
 static __global__ void __launch_bounds__(128) k_assemble_q1(LevelGeom g, const double* __restrict__ cells, int from_log,
                                                      double sigma, double h, double* __restrict__ A,
                                                      int8_t* __restrict__ S) {
