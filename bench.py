@@ -366,7 +366,8 @@ def run_ours(a):
         torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1) / a.steps
-    launches = (G.launches - launches0) // a.steps
+    launches_total = G.launches - launches0
+    launches = launches_total // a.steps
     clocks = clk.summary()
     ms = max_over_ranks(ms)
     final_relres = rr
@@ -457,7 +458,7 @@ def run_ours(a):
                          "kernel": ("k_gs_colour<double> level 0" if a.smoother == "mc8"
                                     else "k_gs_plane<double> level 0 (per colour-sized share of a sweep)"),
                          "peak_source": peak_kind, "launch_ms": launch_ms},
-            "gpu_launches": launches,
+            "gpu_launches": launches_total, "gpu_launches_per_step": launches,
             "clocks": clocks,
             "mixed": mixed,
             "cpu_baseline": cpu,
