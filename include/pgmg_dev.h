@@ -219,6 +219,11 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           bulk prefetches at the start of each pass; 0 =
  *                           off (default).  Same results.  No counterpart in
  *                           the reference.
+ *   PGMG_OPT_GS_BLOCK_LEVELS threads per block of the colour sweep per level:
+ *                           2 bits per level 1..15 (level l at bits 2l-2 and
+ *                           2l-1): 0 = PGMG_OPT_GS_BLOCK (default), 1, 2, 3 =
+ *                           128, 256, 512.  Same results.  No counterpart in
+ *                           the reference.
  *   PGMG_OPT_LU_INVERSE_BAND 1 (default) = the explicit coarse inverse is
  *                           computed one warp per column over the factors'
  *                           band (where it is at most 256 rows on either side
@@ -247,7 +252,8 @@ enum {
     PGMG_OPT_GS_TMA = 19,
     PGMG_OPT_RAT_TILE = 20,
     PGMG_OPT_GS_L2_PREFETCH = 21,
-    PGMG_OPT_LU_INVERSE_BAND = 22
+    PGMG_OPT_LU_INVERSE_BAND = 22,
+    PGMG_OPT_GS_BLOCK_LEVELS = 23
 };
 pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
 /* Autotuner (no counterpart in the reference).  Times `reps` V-cycles (after
@@ -255,7 +261,7 @@ pgmg_status pgmg_dev_set_option(pgmg_handle *h, int key, long long value);
  * options that change no result -- PGMG_OPT_GS_BLOCK, PGMG_OPT_CLUSTER_FIRST,
  * PGMG_OPT_GS_ALTERNATE, PGMG_OPT_GS_PREFETCH, PGMG_OPT_GS_VECTOR, PGMG_OPT_CLUSTER_SIZE,
  * PGMG_OPT_GRID_MAX, PGMG_OPT_PDL, PGMG_OPT_FUSED_RESTRICT, PGMG_OPT_GS_TMA,
- * PGMG_OPT_GS_L2_PREFETCH --
+ * PGMG_OPT_GS_L2_PREFETCH, PGMG_OPT_GS_BLOCK_LEVELS --
  * one at a time from the best so
  * far, and keeps the fastest.  The level-0 solution is saved and restored.
  * The choice is remembered for the process per (grid, periodic axes,

@@ -43,6 +43,7 @@ OPT_GS_TMA = 19
 OPT_RAT_TILE = 20
 OPT_GS_L2_PREFETCH = 21
 OPT_LU_INVERSE_BAND = 22
+OPT_GS_BLOCK_LEVELS = 23
 
 _STATUS = {
     0: "ok", 1: "file error", 2: "memory error", 3: "internal error", 4: "multigrid error",
@@ -294,7 +295,7 @@ class Multigrid:
                      "pdl": OPT_PDL, "grid_max": OPT_GRID_MAX, "gs_vector": OPT_GS_VECTOR,
                      "gs_alternate": OPT_GS_ALTERNATE, "gs_prefetch": OPT_GS_PREFETCH,
                      "fused_restrict": OPT_FUSED_RESTRICT, "gs_tma": OPT_GS_TMA,
-                     "gs_l2_prefetch": OPT_GS_L2_PREFETCH}
+                     "gs_l2_prefetch": OPT_GS_L2_PREFETCH, "gs_block_levels": OPT_GS_BLOCK_LEVELS}
 
     def autotune(self, reps: int = 3, cache: str = None) -> dict:
         """Times V-cycles under the result-neutral execution options and keeps

@@ -170,6 +170,14 @@ pgmg_status check_grid(pgmg_handle* h) {
     return fail(h, PGMG_ERR_TIMEOUT, "an mbarrier wait of the TMA colour pass ran out of time");
 }
 
+// Threads per block of level l's colour sweep (PGMG_OPT_GS_BLOCK, or the
+// level's own PGMG_OPT_GS_BLOCK_LEVELS entry).
+int sweep_block(const pgmg_handle* h, int l) {
+    if (l < 1 || l > 15) return h->gs_block;
+    const int code = (int)((h->gs_block_lv >> (2 * (l - 1))) & 3);
+    return code == 0 ? h->gs_block : code == 1 ? 128 : code == 2 ? 256 : 512;
+}
+
 // One colour pass of k_gs_colour_tma (128 threads per CTA when the sweep
 // block is 128, else 256).
 template <class T>
@@ -192,6 +200,7 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
     Level& L = h->L[l];
     View<T> v = view<T>(L);
     const LevelGeom& g = L.g;
+    const int bs = sweep_block(h, l);
     // An odd periodic axis (possible on the bottom level only) has no valid
     // 8-colouring: sweep that level lexicographically.
     if (g.prd && ((px(g) && (g.m & 1)) || (py(g) && (g.n & 1)) || (pz(g) && (g.o & 1))))
@@ -248,9 +257,9 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                 for (int cc = 0; cc < 8; cc++) {
                     int col = colour_seq(pass ? 7 - cc : cc);
                     int rev = h->gs_alt ? (cc & 1) : 0;
-                    if (h->gs_block == 128)
+                    if (bs == 128)
                         LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col, rev);
-                    else if (h->gs_block == 512)
+                    else if (bs == 512)
                         LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col, rev);
                     else
                         LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col, rev);
@@ -284,9 +293,9 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
             int col = colour_seq(cc < 8 ? cc : 15 - cc);
             int nx = st + 1 < total && l2pf ? colour_seq((st + 1) % per < 8 ? (st + 1) % per : 15 - (st + 1) % per) : -1;
             int rev = h->gs_alt ? (cc & 1) : 0;
-            if (h->gs_block == 128)
+            if (bs == 128)
                 LAUNCH(nblk(nc, 128), 128, k_gs_colour_pf<T, 128>, g, v.x, v.r, v.A, col, rev, nx);
-            else if (h->gs_block == 512)
+            else if (bs == 512)
                 LAUNCH(nblk(nc, 512), 512, k_gs_colour_pf<T, 512>, g, v.x, v.r, v.A, col, rev, nx);
             else
                 LAUNCH(nblk(nc, 256), 256, k_gs_colour_pf<T, 256>, g, v.x, v.r, v.A, col, rev, nx);
@@ -304,10 +313,10 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
                     int rev = h->gs_alt ? (cc & 1) : 0;  // alternate the traversal direction
                     if (g.prd)
                         LAUNCH(nblk(np), kBlock, k_gs_colour<T, true, true>, g, v.x, v.r, v.A, col, k2lo, k2hi, rev);
-                    else if (h->gs_block == 128)
+                    else if (bs == 128)
                         LAUNCH(nblk(np, 128), 128, k_gs_colour<T, true, false, 128>, g, v.x, v.r, v.A, col, k2lo,
                                k2hi, rev);
-                    else if (h->gs_block == 512)
+                    else if (bs == 512)
                         LAUNCH(nblk(np, 512), 512, k_gs_colour<T, true, false, 512>, g, v.x, v.r, v.A, col, k2lo,
                                k2hi, rev);
                     else
@@ -1007,6 +1016,10 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
         case PGMG_OPT_LU_INVERSE_BAND:
             h->lu_inv_band = value != 0;
             break;
+        case PGMG_OPT_GS_BLOCK_LEVELS:
+            if (value < 0 || value >= (1LL << 30)) return fail(h, PGMG_ERR_ARG, "gs_block_levels: 2 bits per level 1..15");
+            h->gs_block_lv = value;
+            break;
         case PGMG_OPT_GS_TMA:
             if (value < 0) return fail(h, PGMG_ERR_ARG, "gs_tma must be >= 0");
             h->gs_tma = value;
@@ -1072,6 +1085,7 @@ pgmg_status pgmg_dev_get_option(pgmg_handle* h, int key, long long* value) {
         case PGMG_OPT_FUSED_RESTRICT: *value = h->fused_restrict; return PGMG_OK;
         case PGMG_OPT_LU_WINDOW: *value = h->lu_window; return PGMG_OK;
         case PGMG_OPT_LU_INVERSE_BAND: *value = h->lu_inv_band; return PGMG_OK;
+        case PGMG_OPT_GS_BLOCK_LEVELS: *value = h->gs_block_lv; return PGMG_OK;
         case PGMG_OPT_GS_TMA: *value = h->gs_tma; return PGMG_OK;
         case PGMG_OPT_RAT_TILE: *value = h->rat_tile; return PGMG_OK;
         case PGMG_OPT_GS_L2_PREFETCH: *value = h->gs_l2pf; return PGMG_OK;
@@ -1448,6 +1462,7 @@ struct TuneVal {
     int fused_restrict;
     long long gs_tma;
     long long gs_l2pf;
+    long long gs_block_lv;
     double ms;
 };
 std::mutex g_tune_mu;
@@ -1465,6 +1480,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->fused_restrict = v.fused_restrict != 0;
     h->gs_tma = v.gs_tma;
     h->gs_l2pf = v.gs_l2pf;
+    h->gs_block_lv = v.gs_block_lv;
     drop_graphs(h);
 }
 
@@ -1572,7 +1588,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     CK(cudaEventCreate(&e1));
     TuneVal best{h->gs_block,         h->coarse_first,   h->cluster_size, h->pdl ? 1 : 0,
                  h->grid_max,         h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch,
-                 h->fused_restrict ? 1 : 0, h->gs_tma, h->gs_l2pf, 0};
+                 h->fused_restrict ? 1 : 0, h->gs_tma, h->gs_l2pf, h->gs_block_lv, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
@@ -1655,6 +1671,23 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
                 if ((st = trial(c)) != PGMG_OK) break;
             }
         }
+    }
+    // Block size per swept level above the cluster tail (a level's best can
+    // differ from level 0's: at 257^3 FP64, 512 threads on 129^3 and 128 on
+    // 33^3).
+    if (st == PGMG_OK && mc8 && !h->prd) {
+        const int top = best.coarse_first < h->nl ? best.coarse_first : h->nl;
+        for (int l = 1; l < top && l <= 15 && st == PGMG_OK; l++)
+            for (int code = 1; code <= 3 && st == PGMG_OK; code++) {
+                const int sh = 2 * (l - 1);
+                const int cur = (int)((best.gs_block_lv >> sh) & 3);
+                const int size = code == 1 ? 128 : code == 2 ? 256 : 512;
+                const int cur_size = cur == 0 ? best.gs_block : cur == 1 ? 128 : cur == 2 ? 256 : 512;
+                if (size == cur_size) continue;
+                TuneVal c = best;
+                c.gs_block_lv = (best.gs_block_lv & ~(3LL << sh)) | ((long long)code << sh);
+                st = trial(c);
+            }
     }
     if (st == PGMG_OK && mc8 && !h->prd && h->grid_blocks[0] > 0 && h->grid_blocks[1] > 0) {
         long long g0 = best.grid_max;

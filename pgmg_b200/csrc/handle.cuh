@@ -185,6 +185,9 @@ struct pgmg_handle {
     // k_gs_colour_pf levels of at most gs_l2pf points prefetch the next
     // pass's stencils into L2 (0 = off).
     long long gs_l2pf = 0;
+    // Per-level block sizes of the colour sweep: 2 bits per level 1..15
+    // (bits 2l-2, 2l-1): 0 = gs_block, 1/2/3 = 128/256/512 threads.
+    long long gs_block_lv = 0;
     int inner_digits = pgmg::kInnerDigits;  // mixed precision: reduction asked of one refinement step (ir_inner_cycles)
     // Persistent whole-GPU sweeps (k_sweeps_grid) for levels above the
     // cluster levels with at most grid_max points (0 = off); co-resident

@@ -384,3 +384,25 @@ def test_lu_inverse_band_same_inverse(case):
         assert np.array_equal(hs[0].get_x(0), hs[1].get_x(0))
     for G in hs:
         G.close()
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+@pytest.mark.parametrize("pattern", [0b110110, 0b011011, 0b111001])
+def test_gs_block_levels_bitwise(precision, pattern):
+    """Per-level block sizes of the colour sweep (2 bits per level) give the
+    default sweep's iterates bit for bit; the option round-trips."""
+    mno = (129, 97, 65)
+    A = make(mno, precision)
+    B = make(mno, precision)
+    B.set_option(P.OPT_CLUSTER_FIRST, B.nlevels)  # every level swept by launches
+    A.set_option(P.OPT_CLUSTER_FIRST, A.nlevels)
+    B.set_option(P.OPT_GS_BLOCK_LEVELS, pattern)
+    assert B.get_option(P.OPT_GS_BLOCK_LEVELS) == pattern
+    for _ in range(2):
+        A.v_cycle(0)
+        B.v_cycle(0)
+        assert np.array_equal(A.get_x(0), B.get_x(0))
+    A.clear_x(0)
+    B.clear_x(0)
+    assert A.solve(1e-10, 100, 0) == B.solve(1e-10, 100, 0)
+    assert np.array_equal(A.get_x(0), B.get_x(0))
