@@ -2016,7 +2016,11 @@ pgmg_status pgmg_dev_solve_io(pgmg_handle* h, const double* r, double* x, double
     k_nat_to_cm<double><<<nblk(g.npts), kBlock, 0, h->stream>>>(g, h->stage, L0.r64);
     CKL();
     TRY(pgmg_dev_clear_x(h, 0));
-    return solve_core(h, tol, max_cycles, check_every, cycles, relres, x);
+    const pgmg_status st = solve_core(h, tol, max_cycles, check_every, cycles, relres, x);
+    // On an error return too, no copy into the caller's buffer may still be
+    // in flight.
+    if (st != PGMG_OK && cudaStreamSynchronize(h->ostream) != cudaSuccess) cudaGetLastError();
+    return st;
 }
 
 }  // extern "C"
