@@ -148,9 +148,12 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           launches.  No counterpart in the reference.
  *   PGMG_OPT_GS_VECTOR      1 = the 8-colour sweep kernel updates 2 (FP64) or
  *                           4 (FP32) consecutive colour points per thread with
- *                           128-bit loads of their stencil coefficients; 0 =
- *                           one point per thread (default).  No counterpart in
- *                           the reference.
+ *                           128-bit loads of their stencil coefficients; 2 = 2
+ *                           points per thread (64-bit loads in FP32; as 1 in
+ *                           FP64); 0 = one point per thread (default).  Only
+ *                           on levels that the TMA, persistent-grid and
+ *                           stencil-prefetch passes do not take.  Same
+ *                           results.  No counterpart in the reference.
  *   PGMG_OPT_GS_ALTERNATE   1 = consecutive colour passes traverse the level in
  *                           opposite directions, so that each starts on the
  *                           solution planes the previous one left in L2
@@ -169,7 +172,7 @@ pgmg_status pgmg_dev_launch_count(pgmg_handle *h, long long *n);
  *                           waiting for the previous kernel (with PGMG_OPT_PDL,
  *                           so that the loads overlap that kernel's drain);
  *                           0 = no level.  Default 4194304.  Levels that
- *                           PGMG_OPT_GS_VECTOR or PGMG_OPT_GRID_MAX sweep keep
+ *                           PGMG_OPT_GS_TMA or PGMG_OPT_GRID_MAX sweep keep
  *                           those paths.  No counterpart in the reference.
  *   PGMG_OPT_INNER_DIGITS   mixed precision, adaptive schedule: the FP32
  *                           V-cycles of one refinement step are asked for at

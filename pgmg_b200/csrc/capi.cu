@@ -248,24 +248,6 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
         return PGMG_OK;
     }
     int S = slab_count(g, (int)sizeof(T), h->slab_budget);
-    if (S == 1 && !g.prd && h->gs_vec) {
-        // 16-byte vector loads, V colour points per thread.
-        constexpr int V = 16 / sizeof(T);
-        long nthr = ((long)g.M2 * g.N2 * g.O2 + V - 1) / V;
-        for (int s = 0; s < sweeps; s++)
-            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
-                for (int cc = 0; cc < 8; cc++) {
-                    int col = colour_seq(pass ? 7 - cc : cc);
-                    int rev = h->gs_alt ? (cc & 1) : 0;
-                    if (bs == 128)
-                        LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col, rev);
-                    else if (bs == 512)
-                        LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col, rev);
-                    else
-                        LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col, rev);
-                }
-        return PGMG_OK;
-    }
     if (S == 1 && !g.prd && h->gs_tma > 0 && g.npts <= h->gs_tma) {
         // Stencils and sources staged by bulk copies (k_gs_colour_tma).
         long nc = (long)g.M2 * g.N2 * g.O2;
@@ -300,6 +282,37 @@ pgmg_status gs_level(pgmg_handle* h, int l, int mode, int smoother, int sweeps =
             else
                 LAUNCH(nblk(nc, 256), 256, k_gs_colour_pf<T, 256>, g, v.x, v.r, v.A, col, rev, nx);
         }
+        return PGMG_OK;
+    }
+    if (S == 1 && !g.prd && h->gs_vec) {
+        // Vector loads, V colour points per thread: 16-byte vectors
+        // (gs_vec 1), or 2 points per thread (gs_vec 2: 8-byte vectors of
+        // FP32; for FP64 the same as 1).  On the levels the variants above
+        // do not take (with the default thresholds, level 0 of a large grid).
+        constexpr int V16 = 16 / sizeof(T);
+        const int V = h->gs_vec == 2 ? 2 : V16;
+        long nthr = ((long)g.M2 * g.N2 * g.O2 + V - 1) / V;
+        for (int s = 0; s < sweeps; s++)
+            for (int pass = 0; pass < (mode ? 2 : 1); pass++)
+                for (int cc = 0; cc < 8; cc++) {
+                    int col = colour_seq(pass ? 7 - cc : cc);
+                    int rev = h->gs_alt ? (cc & 1) : 0;
+                    if (V == V16) {
+                        if (bs == 128)
+                            LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128>, g, v.x, v.r, v.A, col, rev);
+                        else if (bs == 512)
+                            LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512>, g, v.x, v.r, v.A, col, rev);
+                        else
+                            LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256>, g, v.x, v.r, v.A, col, rev);
+                    } else {
+                        if (bs == 128)
+                            LAUNCH(nblk(nthr, 128), 128, k_gs_colour_v<T, 128, 2>, g, v.x, v.r, v.A, col, rev);
+                        else if (bs == 512)
+                            LAUNCH(nblk(nthr, 512), 512, k_gs_colour_v<T, 512, 2>, g, v.x, v.r, v.A, col, rev);
+                        else
+                            LAUNCH(nblk(nthr, 256), 256, k_gs_colour_v<T, 256, 2>, g, v.x, v.r, v.A, col, rev);
+                    }
+                }
         return PGMG_OK;
     }
     for (int s = 0; s < sweeps; s++)
@@ -999,7 +1012,8 @@ pgmg_status pgmg_dev_set_option(pgmg_handle* h, int key, long long value) {
             h->pdl = value != 0;
             break;
         case PGMG_OPT_GS_VECTOR:
-            h->gs_vec = value != 0;
+            if (value < 0 || value > 2) return fail(h, PGMG_ERR_ARG, "gs_vector must be 0, 1 or 2");
+            h->gs_vec = (int)value;
             break;
         case PGMG_OPT_GS_ALTERNATE:
             h->gs_alt = value != 0;
@@ -1474,7 +1488,7 @@ void apply_tuning(pgmg_handle* h, const TuneVal& v) {
     h->cluster_size = v.cluster_size;
     h->pdl = v.pdl != 0;
     h->grid_max = v.grid_max;
-    h->gs_vec = v.gs_vec != 0;
+    h->gs_vec = v.gs_vec;
     h->gs_alt = v.gs_alt != 0;
     h->gs_prefetch = v.gs_prefetch;
     h->fused_restrict = v.fused_restrict != 0;
@@ -1587,7 +1601,7 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     TuneVal best{h->gs_block,         h->coarse_first,   h->cluster_size, h->pdl ? 1 : 0,
-                 h->grid_max,         h->gs_vec ? 1 : 0, h->gs_alt ? 1 : 0, h->gs_prefetch,
+                 h->grid_max,         h->gs_vec,         h->gs_alt ? 1 : 0, h->gs_prefetch,
                  h->fused_restrict ? 1 : 0, h->gs_tma, h->gs_l2pf, h->gs_block_lv, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
     auto trial = [&](TuneVal c) -> pgmg_status {
@@ -1617,9 +1631,15 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
         }
     }
     if (st == PGMG_OK && mc8 && !h->prd) {
-        TuneVal c = best;
-        c.gs_vec = !best.gs_vec;
-        st = trial(c);
+        // 2 points per thread differs from 16-byte vectors only in FP32.
+        const int vmax = h->dims.precision == PGMG_MIXED ? 2 : 1;
+        const int v0 = best.gs_vec;
+        for (int vv = 0; vv <= vmax && st == PGMG_OK; vv++) {
+            if (vv == v0) continue;
+            TuneVal c = best;
+            c.gs_vec = vv;
+            st = trial(c);
+        }
     }
     if (st == PGMG_OK && mc8 && !h->prd) {
         long long q0 = best.gs_l2pf;

@@ -155,7 +155,7 @@ struct pgmg_handle {
     int prd = 0;      // periodic axes of the problem (bit 0 x, 1 y, 2 z)
     bool pdl = true;
     int gs_block = 256;  // threads per block of the colour sweep
-    bool gs_vec = false;  // colour sweep with 16-byte vector loads (k_gs_colour_v)
+    int gs_vec = 0;  // colour sweep with vector loads (k_gs_colour_v): 1 = 16-byte, 2 = 2 points per thread
     bool gs_alt = true;   // colour passes alternate their traversal direction
     // 8-colour levels of at most gs_prefetch points load their stencil before
     // the launch dependency (k_gs_colour_pf); 0 = none.  On the largest

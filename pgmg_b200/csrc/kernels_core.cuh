@@ -78,10 +78,9 @@ __global__ void __launch_bounds__(BS) k_gs_colour(LevelGeom g, T* x, const T* __
 // order, so results are bit-identical to k_gs_colour.  One slab only (p
 // starts at 0, so every thread's first point is a multiple of V and its loads
 // are aligned: colour-major planes are padded to multiples of 64 points).
-template <class T, int BS>
+template <class T, int BS, int V = 16 / sizeof(T)>
 __global__ void __launch_bounds__(BS) k_gs_colour_v(LevelGeom g, T* x, const T* __restrict__ r,
                                                     const T* __restrict__ A, int col, int rev) {
-    constexpr int V = 16 / sizeof(T);
     pdl_enter();
     long nc = (long)g.M2 * g.N2 * g.O2;
     unsigned b = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;

@@ -322,6 +322,11 @@ __device__ __forceinline__ void ld_stream_v(const double* a, uint64_t pol, doubl
     asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
         : "=d"(v[0]), "=d"(v[1]) : "l"(a), "l"(pol));
 }
+// 64-bit streaming loads of 2 floats (8-byte aligned).
+__device__ __forceinline__ void ld_stream_v(const float* a, uint64_t pol, float (&v)[2]) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+        : "=f"(v[0]), "=f"(v[1]) : "l"(a), "l"(pol));
+}
 __device__ __forceinline__ void ld_stream_v(const float* a, uint64_t pol, float (&v)[4]) {
     asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
         : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(a), "l"(pol));

@@ -87,12 +87,15 @@ def test_grid_sweeps_solve_bitwise(precision):
 
 @pytest.mark.parametrize("mno", [(41, 41, 41), (33, 40, 17), (65, 20, 9)])
 @pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
-def test_gs_vector_bitwise(mno, precision):
-    """The 16-byte-load colour sweep (2 or 4 points per thread) gives the
-    one-point-per-thread sweep's iterates bit for bit, odd sizes included."""
+@pytest.mark.parametrize("vec", [1, 2])
+def test_gs_vector_bitwise(mno, precision, vec):
+    """The vector-load colour sweeps (16-byte loads: 2 or 4 points per
+    thread; or 2 points per thread) give the one-point-per-thread sweep's
+    iterates bit for bit, odd sizes included."""
     A = make(mno, precision)
     B = make(mno, precision)
-    B.set_option(P.OPT_GS_VECTOR, 1)
+    B.set_option(P.OPT_GS_VECTOR, vec)
+    assert B.get_option(P.OPT_GS_VECTOR) == vec
     for _ in range(2):
         A.v_cycle(0)
         B.v_cycle(0)
