@@ -1604,12 +1604,27 @@ pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
                  h->grid_max,         h->gs_vec,         h->gs_alt ? 1 : 0, h->gs_prefetch,
                  h->fused_restrict ? 1 : 0, h->gs_tma, h->gs_l2pf, h->gs_block_lv, 0};
     pgmg_status st = time_vcycles(h, reps, e0, e1, &best.ms);
+    // A candidate that times faster than the best so far is timed once more,
+    // and so is the best, each keeping its faster time: the options differ
+    // by a percent or two where they differ at all, about the run-to-run
+    // spread of one timing.
     auto trial = [&](TuneVal c) -> pgmg_status {
         apply_tuning(h, c);
         double t = 0;
         pgmg_status s2 = time_vcycles(h, reps, e0, e1, &t);
         if (s2 == PGMG_ERR_TIMEOUT) return PGMG_OK;  // a candidate that fails is not kept
         if (s2 != PGMG_OK) return s2;
+        if (t < best.ms) {
+            double tb = 0, tc = 0;
+            apply_tuning(h, best);
+            if ((s2 = time_vcycles(h, reps, e0, e1, &tb)) != PGMG_OK) return s2;
+            apply_tuning(h, c);
+            s2 = time_vcycles(h, reps, e0, e1, &tc);
+            if (s2 == PGMG_ERR_TIMEOUT) return PGMG_OK;
+            if (s2 != PGMG_OK) return s2;
+            if (tb < best.ms) best.ms = tb;
+            if (tc < t) t = tc;
+        }
         c.ms = t;
         if (t < best.ms) best = c;
         return PGMG_OK;
