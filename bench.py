@@ -1068,8 +1068,21 @@ def run_profile_mixed(a):
     print(json.dumps({"workload": "mixed only", "value": t, "cycles": cyc, "relres": rr}))
 
 
+def results_only_on_stdout():
+    """Keep the process's standard output for the JSON result lines: file
+    descriptor 1 is pointed at standard error, so that what native code
+    prints with printf (the reference prints its grid hierarchy and its LU
+    fallback notice) goes there, and Python's sys.stdout writes to the
+    original standard output."""
+    sys.stdout.flush()
+    keep = os.dup(1)
+    os.dup2(2, 1)
+    sys.stdout = os.fdopen(keep, "w", buffering=1)
+
+
 def main():
     a = parse()
+    results_only_on_stdout()
     if a.impl == "reference":
         run_reference(a)
     elif a.workload == "small65":

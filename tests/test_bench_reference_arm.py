@@ -19,8 +19,9 @@ def test_reference_arm_json_line():
     out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--size", "33", "--steps", "2",
                           "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
-    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
-    assert len(lines) == 1
+    lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
+    # the reference's own printf output (grid hierarchy) goes to stderr
+    assert len(lines) == 1 and lines[0].startswith("{"), out.stdout[-2000:]
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "s/solve" and d["higher_is_better"] is False
     assert d["steps"] == 2 and d["warmup"] == 1 and d["value"] > 0
