@@ -1058,6 +1058,7 @@ def run_profile_mixed(a):
     G.setup_matrices(coef, S)
     G.setup_fields(r)
     del coef, S
+    G.autotune(cache=a.tune_cache)  # the options the benchmark's mixed leg runs with
 
     def solve():
         G.clear_x(0)

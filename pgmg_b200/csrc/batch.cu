@@ -640,6 +640,7 @@ pgmg_status run_step(pgmg_batch* b, double tol, int max_cycles) {
 
 template <class T>
 pgmg_status batch_step(pgmg_batch* b, double tol, int max_cycles, int* n_active) {
+    TraceRange tr("pgmg batch step");
     if (b->dirty) {
         BTRY(build_shape<T>(b));
         b->stable_steps = 0;
@@ -874,6 +875,7 @@ pgmg_status pgmg_batch_set_option(pgmg_batch* b, int key, long long value) {
 
 pgmg_status pgmg_batch_solve(pgmg_batch* b, double tol, int max_cycles, int* cycles, double* relres) {
     if (!b || max_cycles < 0) return PGMG_ERR_ARG;
+    TraceRange tr("pgmg batch solve");
     // Work of the attached handles issued on their own streams must be done.
     for (pgmg_handle* h : b->slots)
         if (h) BCK(cudaStreamSynchronize(h->stream));

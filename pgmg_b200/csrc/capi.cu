@@ -578,6 +578,7 @@ void drop_graphs(pgmg_handle* h) {
 // small launches of the coarse levels cost no host launch overhead.
 template <class T>
 pgmg_status run_vcycle(pgmg_handle* h, int mode, int smoother) {
+    TraceRange tr(std::is_same<T, float>::value ? "pgmg V-cycle fp32" : "pgmg V-cycle fp64");
     if (!h->use_graphs) return vcycle_t<T>(h, mode, smoother);
     int a = std::is_same<T, float>::value ? 1 : 0, b = mode ? 1 : 0, c = smoother == PGMG_SMOOTH_LEX ? 1 : 0;
     cudaGraphExec_t& ex = h->vgraph[a][b][c];
@@ -703,6 +704,7 @@ pgmg_status ir_step(pgmg_handle* h, int mode, int smoother, double* res2, double
 }
 
 pgmg_status lu_setup(pgmg_handle* h) {
+    TraceRange tr("pgmg coarse LU");
     h->lu_ok = 0;
     int lb = h->nl - 1;
     Level& L = h->L[lb];
@@ -1134,6 +1136,7 @@ pgmg_status pgmg_dev_memory(pgmg_handle* h, size_t* bytes) {
 
 pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const int* S6) {
     if (!h || !coef27) return PGMG_ERR_ARG;
+    TraceRange tr("pgmg upload_level0");
     Level& L = h->L[0];
     const LevelGeom& g = L.g;
     // Boxes: validate on the host (region.hh:498-506 reads them per point).
@@ -1191,6 +1194,7 @@ pgmg_status pgmg_dev_upload_level0(pgmg_handle* h, const double* coef27, const i
 
 pgmg_status pgmg_dev_assemble_q1(pgmg_handle* h, const double* cells, int from_log, double sigma) {
     if (!h) return PGMG_ERR_ARG;
+    TraceRange tr("pgmg assemble_q1");
     if (h->prd) return fail(h, PGMG_ERR_UNSUPPORTED, "the Q1 generator builds Dirichlet problems only");
     Level& L = h->L[0];
     const LevelGeom& g = L.g;
@@ -1232,6 +1236,7 @@ pgmg_status pgmg_dev_rhs_uniform(pgmg_handle* h, uint64_t seed) {
 
 pgmg_status pgmg_dev_build_rat(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
+    TraceRange tr("pgmg build_rat");
     if (!h->uploaded) return fail(h, PGMG_ERR_SETUP, "level-0 stencils not uploaded");
     drop_graphs(h);
     for (int l = 1; l < h->nl; l++) {
@@ -1577,6 +1582,7 @@ pgmg_status pgmg_dev_tma_check(pgmg_handle* h, int level, int run_out) {
 
 pgmg_status pgmg_dev_autotune(pgmg_handle* h, int reps, double* best_ms) {
     if (!h) return PGMG_ERR_ARG;
+    TraceRange tr("pgmg autotune");
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (reps < 1) reps = 3;
     TuneKey key{h->dims.m, h->dims.n, h->dims.o, h->prd, h->dims.precision, h->dims.smoother, h->device};
@@ -1766,6 +1772,7 @@ pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
     if (smoother < 0) smoother = h->dims.smoother;
+    TraceRange tr("pgmg fmg_cycle");
     h->x0_zero = false;
     // multigrid::fmg_cycle (multigrid.cc:109-134), mode 0.
     int ml = h->nl;
@@ -1789,12 +1796,14 @@ pgmg_status pgmg_dev_fmg_cycle(pgmg_handle* h, int smoother) {
 
 pgmg_status pgmg_dev_norms(pgmg_handle* h, int level, double* res2, double* rhs2) {
     TRY(check_level(h, level));
+    TraceRange tr("pgmg norms");
     return norms64(h, level, res2, rhs2);
 }
 
 pgmg_status pgmg_dev_solve_v_cycles(pgmg_handle* h, double p_scale, int* result, double* res2, int* cycles) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    TraceRange tr("pgmg solve_v_cycles");
     if (!h->tol_set) {
         if (!(p_scale > 0)) return fail(h, PGMG_ERR_SETUP, "solve_v_cycles needs guide.set_tol (p_scale > 0)");
         double eps = 2.220446049250313e-16;
@@ -1878,6 +1887,7 @@ static pgmg_status solve_core(pgmg_handle* h, double tol, int max_cycles, int ch
                               double* relres, double* x_out) {
     if (!h) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    TraceRange tr("pgmg solve");
     if (check_every < 0) check_every = 1;
     int smoother = h->dims.smoother;
     double res2 = 0, rhs2 = 0, rr = INFINITY;
@@ -1896,6 +1906,7 @@ static pgmg_status solve_core(pgmg_handle* h, double tol, int max_cycles, int ch
         // (it is the next correction's source), so it checks every step too.
         bool check = mixed || nc >= next_check || nc >= max_cycles;
         bool zero = nc == 0 && h->x0_zero;  // residual = source: no stencil pass needed
+        TraceRange check_range("pgmg check", check);  // ends once the norms are read
         out_now = false;
         if (x_out && check && !zero) {
             // An FP64 check is scheduled where the solve is predicted to
@@ -1978,8 +1989,10 @@ static pgmg_status solve_core(pgmg_handle* h, double tol, int max_cycles, int ch
             next_check = plan.next(nc, tol);
             if (next_check > max_cycles) next_check = max_cycles;
         }
+        check_range.end();
         h->x0_zero = false;
         if (mixed) {
+            TraceRange step_range("pgmg refinement step");
             // One refinement step: A32 e = r32 solved by `inner` FP32
             // V-cycles from e = 0, then x64 += e.  The count is the number of
             // cycles the check schedule expects to run before its next check;
@@ -2038,6 +2051,7 @@ pgmg_status pgmg_dev_solve_io(pgmg_handle* h, const double* r, double* x, double
                               int check_every, int* cycles, double* relres) {
     if (!h || !r || !x) return PGMG_ERR_ARG;
     if (!h->built) return fail(h, PGMG_ERR_SETUP, "operators not built");
+    TraceRange tr("pgmg solve_io");
     if (!h->ostream) {
         if (cudaStreamCreateWithFlags(&h->ostream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {

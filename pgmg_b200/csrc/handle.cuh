@@ -11,6 +11,7 @@
 #include "kernels_setup.cuh"
 #include "kernels_tma.cuh"
 #include "layout.cuh"
+#include "trace.cuh"
 
 namespace pgmg {
 constexpr int kMaxLevels = 16;      // mg_max_levels, common.hh:15
