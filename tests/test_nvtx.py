@@ -13,7 +13,7 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOOL_SRC = os.path.join(ROOT, "tests", "cpp", "nvtx_record.c")
-CUDA_INC = "/usr/local/cuda/include"
+CUDA_INC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
 
 
 def _build_tool(tmp_path):
