@@ -842,6 +842,40 @@ pgmg_status pgmg_dev_plan_bytes(const pgmg_dims* dims, size_t* bytes) {
     return PGMG_OK;
 }
 
+// Page-locked host pairs for the handles' residual norms (the reduction
+// kernel writes each check's two sums straight into its handle's pair).  They
+// come from blocks of kPinPairs pairs that are allocated once, portable to
+// every device, and reused for the life of the process, so that creating and
+// destroying a handle -- which a server does for every new request -- does
+// not page-lock memory: that allocation is slow, and CUDA lets it serialise
+// the work of concurrent streams.
+constexpr int kPinPairs = 256;
+// (The list is never destroyed, so a handle destroyed during process exit,
+// after static destructors have run, can still return its pair.)
+static std::mutex g_pin_mu;
+static std::vector<double*>& g_pin_free = *new std::vector<double*>;
+
+static double* pin_pair_take() {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) {
+        void* block = nullptr;
+        if (cudaHostAlloc(&block, kPinPairs * 2 * sizeof(double), cudaHostAllocPortable | cudaHostAllocMapped) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (int i = kPinPairs - 1; i >= 0; i--) g_pin_free.push_back(static_cast<double*>(block) + 2 * i);
+    }
+    double* p = g_pin_free.back();
+    g_pin_free.pop_back();
+    return p;
+}
+
+static void pin_pair_give(double* p) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+
 static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_bytes, pgmg_handle** out) {
     if (!dims || !out) return PGMG_ERR_ARG;
     *out = nullptr;
@@ -897,11 +931,11 @@ static pgmg_status create_common(const pgmg_dims* dims, void* mem, size_t mem_by
         return PGMG_ERR_CUDA;
     }
     h->stream = h->own;
-    if (cudaMallocHost(&h->norm_pin, 2 * sizeof(double)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_pre, cudaEventDisableTiming) != cudaSuccess ||
+    h->norm_pin = pin_pair_take();
+    if (!h->norm_pin || cudaEventCreateWithFlags(&h->ev_pre, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_post, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
-        if (h->norm_pin) cudaFreeHost(h->norm_pin);
+        if (h->norm_pin) pin_pair_give(h->norm_pin);
         h->norm_pin = nullptr;  // checks fall back to a copy and a stream synchronisation
     }
     for (int size : {16, 8}) {
@@ -957,7 +991,7 @@ pgmg_status pgmg_dev_destroy(pgmg_handle* h) {
     if (!h) return PGMG_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    if (h->norm_pin) cudaFreeHost(h->norm_pin);
+    if (h->norm_pin) pin_pair_give(h->norm_pin);
     if (h->ev_pre) cudaEventDestroy(h->ev_pre);
     if (h->ev_post) cudaEventDestroy(h->ev_post);
     if (h->ostream) cudaStreamSynchronize(h->ostream);
